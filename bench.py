@@ -1,0 +1,423 @@
+#!/usr/bin/env python
+"""Training-step throughput of the QSDVR render path on B200 (rays/s, fwd+bwd).
+
+Workload (default ``plain256``): 256^3 quadric grid + [(257)^3, 32] appearance grid, fp32,
+100 seeded views at 800x800 (focal 1111.1 px, upper hemisphere at radius 4.03), 65536
+random rays per step, 256 samples/ray over t in [2, 6] (interval 4/256).  Targets are
+rendered from a seeded procedural ground-truth scene.  One step = zero the gradient
+buffers + one fused forward + MSE + backward launch over the batch; inputs (2.7 GB of
+grids) are far larger than L2, so no flush is needed between steps.
+
+``--impl reference`` times the reference's own CPU path (its pure-torch renderer with the
+per-ray compositing loop, restated to run on the host) on a bounded sample of the same
+workload and prints the same JSON line with "impl": "reference".
+
+Launch: python bench.py [--gpus N --steps K --warmup W]; for N > 1 under torchrun (one
+replica per GPU, each with its own batches: weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: grid R, rays/step, views, image size, focal, camera radius, interval, storage
+    "plain256": dict(R=256, rays=65536, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
+                     storage="f32"),
+    "bf16_256": dict(R=256, rays=65536, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
+                     storage="bf16"),
+    "plain128": dict(R=128, rays=8192, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
+                     storage="f32"),
+}
+BYTES_PER_SAMPLE = {"f32": 3264, "bf16": 2240}  # algorithmic bytes per render sample (3-pass model)
+BYTES_PER_RAY = 64  # origin + dir in, target in, colour out, RayInfo
+K_LOGISTIC = 5.0
+METRIC = "train rays/s fwd+bwd @256^3 grid (256 samples/ray, 65536-ray batches)"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic_per_sample(storage: str):
+    """DRAM bytes per render sample of the train kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "fused_train_dram.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith(f"dram_bytes_per_render_sample_{storage}:"):
+                    return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------------------- setup
+
+def build_scene(cfg, device, seed):
+    """Ground-truth scene (targets), trained model, and the ray tables of all views."""
+    from qsdvr_b200 import fused, scenes
+    from qsdvr_b200.camera import Camera
+
+    R = cfg["R"]
+    gt_sdf = fused.pad_grid7(scenes.procedural_grid(R, seed=seed, device=device).reshape(-1, 7))
+    gt_data = scenes.appearance(R, seed=seed, device=device, procedural=True)
+    sdf = fused.pad_grid7(scenes.sphere_grid(R, 0.5, 0.01, seed=seed, device=device).reshape(-1, 7))
+    data = scenes.appearance(R, seed=seed + 1, device=device)
+    cams = scenes.hemisphere_cameras(cfg["views"], cfg["radius"], cfg["size"], cfg["size"], cfg["focal"], 2.0, 6.0,
+                                     seed=seed)
+    rays, origin, direction = [], [], []
+    mask = torch.ones(cfg["size"] * cfg["size"], dtype=torch.bool)
+    for a in cams:
+        c = Camera(a, cfg["interval"], R, device=device)
+        c.GenerateRayPoints(mask)
+        rays.append(c.rayList)
+        origin.append(c.originList)
+        direction.append(c.dirList)
+    return dict(gt=(gt_sdf, gt_data), model=(sdf, data), rays=torch.cat(rays), origin=torch.cat(origin),
+                dir=torch.cat(direction))
+
+
+def make_batches(scene, cfg, count, device, seed):
+    from qsdvr_b200 import fused
+
+    gen = torch.Generator(device=device).manual_seed(seed)
+    total = scene["rays"].shape[0]
+    out = []
+    for _ in range(count):
+        idx = torch.randint(0, total, (cfg["rays"],), generator=gen, device=device)
+        b = dict(rays=scene["rays"][idx].contiguous(), origin=scene["origin"][idx].contiguous(),
+                 dir=scene["dir"][idx].contiguous())
+        gs, gd = scene["gt"]
+        b["target"] = fused.render_forward(b["rays"], b["origin"], b["dir"], gs, gd, cfg["R"], cfg["interval"],
+                                           K_LOGISTIC, "fixed")
+        out.append(b)
+    return out
+
+
+def samples_of(batch):
+    c = batch["rays"][:, 0].long()
+    return int(torch.clamp(c - 1, min=0).sum())
+
+
+# ----------------------------------------------------------------------------- timing
+
+def time_device(step, steps, warmup, stream):
+    """Warm-up, then K steps between two events; also returns per-step kernel events."""
+    for i in range(warmup):
+        step(i, None)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for i in range(steps):
+        step(i, ev[i])
+    stop.record(stream)
+    torch.cuda.synchronize()
+    total_ms = start.elapsed_time(stop)
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    return total_ms, kern_ms
+
+
+def run_ours(args, cfg, device, ws, rank):
+    from qsdvr_b200 import fused
+
+    R = cfg["R"]
+    storage = cfg["storage"]
+    scene = build_scene(cfg, device, seed=0)
+    batches = make_batches(scene, cfg, 8, device, seed=1000 + rank)
+    sdf, data = scene["model"]
+    transmittance = "log" if storage == "bf16" else "product"
+    if storage == "bf16":
+        sdf_k, data_k = sdf.to(torch.bfloat16), data.to(torch.bfloat16)
+    else:
+        sdf_k, data_k = sdf, data
+    sg = torch.zeros(sdf.shape, dtype=torch.float32, device=device)
+    dg = torch.zeros(data.shape, dtype=torch.float32, device=device)
+    loss = torch.zeros(1, dtype=torch.float32, device=device)
+    color = torch.empty((cfg["rays"], 3), dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    def step(i, ev):
+        b = batches[i % len(batches)]
+        sg.zero_()
+        dg.zero_()
+        loss.zero_()
+        if ev is not None:
+            ev[0].record(stream)
+        fused.render_train(b["target"], b["rays"], b["origin"], b["dir"], sdf_k, data_k, R, cfg["interval"],
+                           K_LOGISTIC, sg, dg, "compat", transmittance, loss=loss, color=color)
+        if ev is not None:
+            ev[1].record(stream)
+
+    if ws > 1:
+        torch.distributed.barrier()
+    with ClockSampler(device.index) as clk:
+        total_ms, kern_ms = time_device(step, args.steps, args.warmup, stream)
+    if ws > 1:
+        torch.distributed.barrier()
+    # ---- e2e through the public API with host buffers (pinned), copies inside the region
+    host = []
+    for b in batches:
+        host.append({k: v.cpu().pin_memory() for k, v in b.items()})
+    dev_in = {k: torch.empty_like(v) for k, v in batches[0].items()}
+    loss_host = torch.zeros(1, dtype=torch.float32).pin_memory()
+    h2d = sum(v.numel() * v.element_size() for v in host[0].values())
+
+    def e2e_step(i, ev):
+        hb = host[i % len(host)]
+        for k, v in hb.items():
+            dev_in[k].copy_(v, non_blocking=True)
+        sg.zero_()
+        dg.zero_()
+        loss.zero_()
+        fused.render_train(dev_in["target"], dev_in["rays"], dev_in["origin"], dev_in["dir"], sdf_k, data_k, R,
+                           cfg["interval"], K_LOGISTIC, sg, dg, "compat", transmittance, loss=loss, color=color)
+        loss_host.copy_(loss, non_blocking=True)
+
+    if ws > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    e2e_ms, _ = time_device(e2e_step, args.steps, args.warmup, stream)
+    wall_e2e = time.perf_counter() - t0
+    # ---- aggregate over ranks (max time)
+    times = torch.tensor([total_ms, e2e_ms, sum(kern_ms) / len(kern_ms)], dtype=torch.float64, device=device)
+    if ws > 1:
+        torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
+    total_ms, e2e_ms, kern_avg = times.tolist()
+    rays_all = cfg["rays"] * args.steps * ws
+    value = rays_all / (total_ms / 1e3)
+    e2e_value = rays_all / (e2e_ms / 1e3)
+    # ---- roofline of the train kernel
+    samples = [samples_of(b) for b in batches]
+    mean_samples = sum(samples) / len(samples)
+    alg_bytes = mean_samples * BYTES_PER_SAMPLE[storage] + cfg["rays"] * BYTES_PER_RAY
+    achieved = alg_bytes / (kern_avg / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    tps = profiled_traffic_per_sample(storage)
+    traffic = None if tps is None else tps * mean_samples
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "rays/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if storage == "f32" else "bf16 storage, f32 math",
+        "data": "synthetic (seeded procedural scene, random-init sphere model)",
+        "config": {"workload": f"{args.workload}: R={R}^3 quadric + ({R + 1})^3x32 appearance grid, {storage}, "
+                               f"{cfg['rays']} random rays/step from {cfg['views']} views at {cfg['size']}^2, "
+                               f"interval {cfg['interval']:.6g} (256 samples/ray), compat mode, k={K_LOGISTIC}",
+                   "global_batch": cfg["rays"] * ws, "samples_per_step": round(mean_samples),
+                   "step": "zero grads + fused forward/MSE/backward launch",
+                   "l2": "inputs larger than L2 (grids 2.7 GB), no flush", "parallelism": f"replicas x{ws}"},
+        "e2e": {"value": round(e2e_value, 1), "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4,
+                "wall_s": round(wall_e2e, 3)},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None if traffic is None else round(traffic),
+                     "kernel": "render_kernel<train>", "kernel_ms": round(kern_avg, 4),
+                     "algorithmic_bytes": round(alg_bytes), "bytes_per_sample": BYTES_PER_SAMPLE[storage],
+                     "peak_kind": peak_kind},
+        "clocks": clk.summary(),
+    }
+    if ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(scene, batches[0], cfg, args.cpu_rays)
+    return out
+
+
+# ----------------------------------------------------------------------------- CPU path
+
+def _cpu_step(grid7, data, batch_cpu, R, interval):
+    """One fwd+bwd of the reference's torch render path on the host (its per-ray loop)."""
+    from oracle.render_torch_cpu import render_torch_cpu
+    from qsdvr_b200.qsdvr import CameraArgs  # noqa: F401  (same package, no GPU use)
+    import oracle.oracle as O
+
+    pts = O.generate_ray_points(batch_cpu["rays"], batch_cpu["origin"], batch_cpu["dir"], interval, R)
+    inp = {k: torch.from_numpy(v) for k, v in pts.items()}
+    inp["rayList"] = torch.from_numpy(batch_cpu["rays_packed"].astype(np.int64))
+    g = grid7.detach().requires_grad_()
+    d = data.detach().requires_grad_()
+    img = render_torch_cpu(g, d, inp, R, K_LOGISTIC)
+    loss = ((img - batch_cpu["target"]) ** 2).mean()
+    loss.backward()
+    return float(loss)
+
+
+def _cpu_batch(batch, n):
+    """First n rays of a batch, repacked with fresh sample offsets (host arrays)."""
+    rays = batch["rays"][:n].cpu().numpy().view(np.uint32).copy()
+    c = rays[:, 0].astype(np.int64)
+    rc = np.maximum(c - 1, 0)
+    rays[:, 1] = np.cumsum(c) - c
+    rays[:, 2] = rc
+    rays[:, 3] = np.cumsum(rc) - rc
+    return dict(rays=rays, rays_packed=rays, origin=batch["origin"][:n].cpu().numpy(),
+                dir=batch["dir"][:n].cpu().numpy(), target=batch["target"][:n].cpu())
+
+
+def cpu_baseline(scene, batch, cfg, n_rays, steps=1):
+    """The reference's CPU path on a bounded sample: n_rays of one batch, fwd+bwd."""
+    sdf, data = scene["model"]
+    grid7 = sdf[:, :7].contiguous().cpu()
+    data_cpu = data.cpu()
+    b = _cpu_batch(batch, n_rays)
+    threads = torch.get_num_threads()
+    _cpu_step(grid7, data_cpu, b, cfg["R"], cfg["interval"])  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        _cpu_step(grid7, data_cpu, b, cfg["R"], cfg["interval"])
+    dt = (time.perf_counter() - t0) / steps
+    return {"value": round(n_rays / dt, 2), "unit": "rays/s", "cores": threads, "kind": "port",
+            "sample": f"{n_rays} rays of one {cfg['rays']}-ray batch ({int(np.maximum(b['rays'][:, 0].astype(np.int64) - 1, 0).sum())} "
+                      f"render samples), fwd+bwd of the reference's torch render path (models/render_torch.py "
+                      f"per-ray loop) on the host, {steps} timed step(s) after 1 warm-up; os.cpu_count()="
+                      f"{os.cpu_count()}"}
+
+
+def run_reference(args, cfg):
+    """The reference's CPU implementation timed on the host cores (rank 0 only)."""
+    torch.set_num_threads(os.cpu_count() or 1)
+    device = torch.device("cuda", 0) if torch.cuda.is_available() else None
+    if device is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no CUDA device to build the synthetic scene"}))
+        return
+    scene = build_scene(cfg, device, seed=0)
+    batch = make_batches(scene, cfg, 1, device, seed=1000)[0]
+    sdf, data = scene["model"]
+    grid7 = sdf[:, :7].contiguous().cpu()
+    data_cpu = data.cpu()
+    del scene
+    b = _cpu_batch(batch, args.cpu_rays)
+    for _ in range(args.warmup):
+        _cpu_step(grid7, data_cpu, b, cfg["R"], cfg["interval"])
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _cpu_step(grid7, data_cpu, b, cfg["R"], cfg["interval"])
+    dt = time.perf_counter() - t0
+    value = args.cpu_rays * args.steps / dt
+    line = {"metric": METRIC, "impl": "reference", "value": round(value, 2), "unit": "rays/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (same seeded scene and batch as the GPU arm)",
+            "config": {"workload": f"{args.workload}: bounded sample of {args.cpu_rays} rays per step of the "
+                                   f"{cfg['rays']}-ray batch", "global_batch": args.cpu_rays},
+            "cpu_baseline": {"value": round(value, 2), "unit": "rays/s", "cores": torch.get_num_threads(),
+                             "kind": "port",
+                             "sample": f"{args.cpu_rays} rays/step, reference torch render path (per-ray loop) "
+                                       f"fwd+bwd on the host"},
+            "e2e": {"value": round(value, 2), "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain256", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-rays", type=int, default=48)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    cfg = WORKLOADS[args.workload]
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, cfg)
+        return
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if ws > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=device)
+    try:
+        out = run_ours(args, cfg, device, ws, rank)
+        if rank == 0:
+            print(json.dumps(out))
+    finally:
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

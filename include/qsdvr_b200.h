@@ -1,0 +1,226 @@
+/*
+ * qsdvr_b200 — C ABI of the B200-native QSDVR render path.
+ *
+ * Every entry point takes plain device pointers, element counts and the caller's CUDA
+ * stream, returns a status code (QSDVR_OK on success) and never allocates: scratch
+ * space is passed in by the caller (query its size with the *_workspace_size
+ * functions).  Gradient buffers that receive atomic accumulation must be zeroed by the
+ * caller, as in the reference.  Kernels check every grid / sample index they derive
+ * from caller data and skip out-of-range accesses, recording the fact in a device
+ * error word (qsdvr_device_error).
+ *
+ * Reference interface replaced by each entry point (paths within the reference project):
+ *   qsdvr pybind module kernel/qsdvr.cpp:5-50, host wrappers in kernel/camera.cu,
+ *   kernel/surface.cu, kernel/render.cu, declarations include/camera.h:57-59,
+ *   include/surface.h:4-14, include/render.h:4-14.
+ */
+#ifndef QSDVR_B200_H
+#define QSDVR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status ---------------------------------------------------------------------- */
+enum {
+    QSDVR_OK = 0,
+    QSDVR_ERR_INVALID_ARGUMENT = 1, /* null pointer, zero/oversized extent, bad mode  */
+    QSDVR_ERR_ALIGNMENT = 2,        /* pointer not aligned as the layout requires     */
+    QSDVR_ERR_WORKSPACE = 3,        /* caller workspace too small                      */
+    QSDVR_ERR_CUDA = 4,             /* a CUDA runtime call or launch failed            */
+    QSDVR_ERR_UNSUPPORTED = 5       /* valid request this build does not implement     */
+};
+
+/* Bits of the device error word. */
+enum {
+    QSDVR_DEVERR_INDEX = 1u,        /* a cell / vertex index outside the grid         */
+    QSDVR_DEVERR_CAPACITY = 2u,     /* a ray's samples run past the sample buffers     */
+    QSDVR_DEVERR_RAY = 4u           /* a ray record is inconsistent (count 1, overflow) */
+};
+
+/* Shading / indexing modes. */
+enum {
+    QSDVR_MODE_COMPAT = 0, /* the reference exactly: overlapping SH reads, sheared vertex index */
+    QSDVR_MODE_FIXED = 1   /* packed SH layout, vertex index x + y(R+1) + z(R+1)^2             */
+};
+
+/* Message for the last non-OK status returned on this host thread. */
+const char *qsdvr_last_error(void);
+/* ABI version (major * 100 + minor). */
+int qsdvr_version(void);
+/* Read (and clear when clear != 0) the device error word of the current device. */
+int qsdvr_device_error(uint32_t *word, int clear, cudaStream_t stream);
+
+/* ---- camera (kernel/camera.cu) ----------------------------------------------------- */
+
+/* 16-byte per-ray record; include/common.h:17-23 (RayInfo), stored as int32 [N,4]. */
+typedef struct qsdvr_ray_info {
+    uint32_t sdf_count;
+    uint32_t sdf_offset;
+    uint32_t render_count;
+    uint32_t render_offset;
+} qsdvr_ray_info;
+
+/* include/camera.h:4-17 (CameraArgs): pixel (px,py) at depth z maps to
+ * R * [(px+cx)/fx*z, (py+cy)/fy*z, z] + t; near/far are camera depths. */
+typedef struct qsdvr_camera {
+    uint32_t width;
+    uint32_t height;
+    float rotation[9];    /* row-major */
+    float translation[3];
+    float fx, fy, cx, cy;
+    float near_depth, far_depth;
+} qsdvr_camera;
+
+size_t qsdvr_ray_cut_workspace_size(uint32_t pixel_count);
+
+/* Replaces RayCut (kernel/camera.cu:98-130, include/camera.h:57).  mask: device uint8
+ * [pixel_count]; rays/origin/dir: [pixel_count] records.  For masked pixels writes the
+ * full record (counts < 2 zeroed, exclusive-scan offsets in pixel order); for unmasked
+ * pixels only sdf_count, as the reference does.  totals (device, 2 x uint32) receives
+ * the total SDF and render sample counts.  Runs entirely on the device. */
+int qsdvr_ray_cut(const qsdvr_camera *camera, const uint8_t *mask, qsdvr_ray_info *rays, float *origin,
+                  float *dir, float interval, uint32_t pixel_count, uint32_t *totals, void *workspace,
+                  size_t workspace_bytes, cudaStream_t stream);
+
+/* Replaces GenerateRayPoints (kernel/camera.cu:132-147, include/camera.h:59).
+ * sdf_capacity / render_capacity are the lengths of the sample lists. */
+int qsdvr_generate_ray_points(const qsdvr_ray_info *rays, const float *origin, const float *dir,
+                              uint32_t ray_count, float interval, uint32_t base_volume_reso,
+                              float *sdf_points, int32_t *sdf_index, float *render_points,
+                              int32_t *render_index, float *view_dir, uint64_t sdf_capacity,
+                              uint64_t render_capacity, cudaStream_t stream);
+
+/* ---- quadric surface grid (kernel/surface.cu) --------------------------------------- */
+
+size_t qsdvr_layer_to_grid_workspace_size(uint32_t reso);
+
+/* Replaces LayerToGridForward (kernel/surface.cu:148-229, include/surface.h:4).
+ * Layers and offset[4] are device arrays; grid7 is [reso^3][7].  The prefix
+ * recurrences run on the device. */
+int qsdvr_layer_to_grid_forward(float *grid7, const float *x_layer, const float *y_layer,
+                                const float *z_layer, const float *offset, uint32_t reso, void *workspace,
+                                size_t workspace_bytes, cudaStream_t stream);
+
+/* Replaces LayerToGridBackward (kernel/surface.cu:231-341, include/surface.h:6).
+ * Writes (not accumulates) x/y/z layer gradients [reso] and offset gradient [4]. */
+int qsdvr_layer_to_grid_backward(const float *grad7, uint32_t reso, float *x_grad, float *y_grad,
+                                 float *z_grad, float *offset_grad, void *workspace, size_t workspace_bytes,
+                                 cudaStream_t stream);
+
+/* Replaces SampleSDFForward (kernel/surface.cu:343-350, include/surface.h:8).
+ * grid7 [cell_count][7], points [count][3], index [count]. */
+int qsdvr_sample_sdf_forward(float *out, const float *grid7, const float *points, const int32_t *index,
+                             uint64_t count, float reso, uint64_t cell_count, cudaStream_t stream);
+
+/* Replaces SampleSDFBackward (kernel/surface.cu:352-359, include/surface.h:10).
+ * Accumulates into grid7_grad (caller zeroes). */
+int qsdvr_sample_sdf_backward(const float *grad_out, const float *grid7, const float *points,
+                              const int32_t *index, float *grid7_grad, uint64_t count, float reso,
+                              uint64_t cell_count, cudaStream_t stream);
+
+/* Replaces SampleNormalForward (kernel/surface.cu:361-367, include/surface.h:12). */
+int qsdvr_sample_normal_forward(float *out, const float *grid7, const float *points, const int32_t *index,
+                                uint64_t count, uint64_t cell_count, cudaStream_t stream);
+
+/* Replaces SampleNormalBackward (kernel/surface.cu:369-375, include/surface.h:14). */
+int qsdvr_sample_normal_backward(const float *grad_out, const float *grid7, const float *points,
+                                 const int32_t *index, float *grid7_grad, uint64_t count, uint64_t cell_count,
+                                 cudaStream_t stream);
+
+/* ---- appearance, shading, compositing (kernel/render.cu) ---------------------------- */
+
+/* Replaces GridInterpolationForward (kernel/render.cu:317-323, include/render.h:4).
+ * data [vertex_count][32]; the corners of sample i are index[i] + {0,1} + {0,reso} +
+ * {0,reso^2} (in vertices), as the reference addresses them; out [count][32]. */
+int qsdvr_grid_interpolation_forward(const float *data, const float *points, const int32_t *index, float *out,
+                                     uint64_t count, uint32_t reso, uint64_t vertex_count, cudaStream_t stream);
+
+/* Replaces GridInterpolationBackward (kernel/render.cu:325-331, include/render.h:6).
+ * Accumulates into data_grad [vertex_count][32] (caller zeroes). */
+int qsdvr_grid_interpolation_backward(float *data_grad, const float *points, const int32_t *index,
+                                      const float *grad_out, uint64_t count, uint32_t reso,
+                                      uint64_t vertex_count, cudaStream_t stream);
+
+/* Replaces ShaderForward (kernel/render.cu:333-339, include/render.h:8).  mode:
+ * QSDVR_MODE_COMPAT reproduces the reference's overlapping SH read. */
+int qsdvr_shader_forward(float *out, const float *normal, const float *view, const float *data,
+                         float *specular, uint64_t count, int mode, cudaStream_t stream);
+
+/* Replaces ShaderBackward (kernel/render.cu:341-347, include/render.h:10). */
+int qsdvr_shader_backward(const float *grad_out, const float *normal, const float *view, const float *data,
+                          const float *specular, float *normal_grad, float *data_grad, uint64_t count, int mode,
+                          cudaStream_t stream);
+
+/* Replaces RayAggregateForward (kernel/render.cu:349-355, include/render.h:12).
+ * out [ray_count][3]; alpha, T [render samples]. */
+int qsdvr_ray_aggregate_forward(float *out, const float *rgb, const float *sdf, const qsdvr_ray_info *rays,
+                                float *alpha, float *transmittance, uint32_t ray_count, float logistic_coef,
+                                uint64_t sdf_capacity, uint64_t render_capacity, cudaStream_t stream);
+
+/* Replaces RayAggregateBackward (kernel/render.cu:357-363, include/render.h:14). */
+int qsdvr_ray_aggregate_backward(const float *grad_out, const float *rgb, const float *sdf,
+                                 const qsdvr_ray_info *rays, const float *alpha, const float *transmittance,
+                                 float *rgb_grad, float *sdf_grad, uint32_t ray_count, float logistic_coef,
+                                 uint64_t sdf_capacity, uint64_t render_capacity, cudaStream_t stream);
+
+
+/* ---- fused render path (B200-native; no reference counterpart as a single kernel) ---- */
+
+enum { QSDVR_STORAGE_F32 = 0, QSDVR_STORAGE_BF16 = 1 };
+enum {
+    QSDVR_TRANSMITTANCE_PRODUCT = 0, /* T_{i+1} = T_i (1 - alpha_i), as the reference        */
+    QSDVR_TRANSMITTANCE_LOG = 1      /* T_i = exp(sum log(1 - alpha)), compensated summation */
+};
+
+/* One batch of rays through the whole render path.  The rays are the reference's
+ * per-ray tables (RayCut output after masking: RayInfo, origin = first in-box sample,
+ * unit direction); samples are generated on the fly exactly as GenerateRayPoints
+ * (kernel/camera.cu:60-96) would.  Only sdf_count of each record is read.
+ *   sdf_grid: [R^3][8] (a0..a6 + one pad) in `storage` precision, cell x + yR + zR^2;
+ *   data:     [(R+1)^3][32] appearance rows in `storage` precision;
+ *   grads:    fp32, same layouts, accumulated with atomics (caller zeroes). */
+typedef struct qsdvr_render_args {
+    const qsdvr_ray_info *rays;
+    const float *origin;      /* [ray_count][3] */
+    const float *dir;         /* [ray_count][3] */
+    uint32_t ray_count;
+    uint32_t reso;            /* R */
+    float interval;           /* sample spacing along the ray */
+    float logistic_coef;      /* k of alpha = max((e^{-k s_{i+1}} - e^{-k s_i}) / (1 + e^{-k s_{i+1}}), 0) */
+    int32_t mode;             /* QSDVR_MODE_* */
+    int32_t storage;          /* QSDVR_STORAGE_* of sdf_grid and data */
+    int32_t transmittance;    /* QSDVR_TRANSMITTANCE_* */
+    int32_t reserved;
+    const void *sdf_grid;
+    const void *data;
+    float *color;             /* [ray_count][3] output of forward / train */
+    const float *target;      /* [ray_count][3] train: MSE target */
+    const float *grad_color;  /* [ray_count][3] backward: dL/dcolor */
+    float *sdf_grad;          /* [R^3][8] accumulated */
+    float *data_grad;         /* [(R+1)^3][32] accumulated */
+    float *loss;              /* train: sum over rays of |color - target|^2 is added here */
+    float grad_scale;         /* train: dL/dcolor = grad_scale * (color - target) */
+} qsdvr_render_args;
+
+/* Replaces RenderGrid.forward (models/render.py:225-234, i.e. the SampleSDF, SampleNormal,
+ * GridInterpolation, Shader and RayAggregate forwards) fused with GenerateRayPoints
+ * (kernel/camera.cu:132-147): writes color. */
+int qsdvr_render_forward(const qsdvr_render_args *args, cudaStream_t stream);
+/* Replaces the backward chain of RenderGrid (models/render.py:27-170: RayAggregate, Shader,
+ * GridInterpolation, SampleNormal, SampleSDF backwards) for a given dL/dcolor; per-sample
+ * alpha and colour are recomputed, nothing per-sample is read from memory. */
+int qsdvr_render_backward(const qsdvr_render_args *args, cudaStream_t stream);
+/* Forward + MSE loss gradient + backward in one launch (test.py:30-33 training step
+ * without the optimizer): writes color, accumulates loss and gradients. */
+int qsdvr_render_train(const qsdvr_render_args *args, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QSDVR_B200_H */

@@ -1,0 +1,605 @@
+// Fused render path: for every ray, sample generation -> quadric SDF and normal ->
+// trilinear 32-channel fetch -> reflection shading -> NeuS alpha -> transmittance ->
+// colour, and the whole backward, in one kernel.  Nothing per-sample is stored in global
+// memory: the backward recomputes each sample (memory stays O(rays)).
+//
+// Work mapping (one warp per ray, 32 render samples per "chunk"):
+//   * lane i owns render sample i of the chunk: its positions (bit-exact with
+//     GenerateRayPoints), quadric cells, SDF values, normal, alpha and shading;
+//   * the 32-channel appearance rows are gathered by groups of 8 lanes (one float4 or
+//     4 x bf16 each), so every load covers whole 128-byte (64-byte bf16) vertex rows,
+//     interpolated and staged in a per-warp shared-memory tile [32][36] floats
+//     (row stride 36 keeps both the row-wise and the lane-wise float4 accesses
+//     conflict-free);
+//   * transmittance is an exclusive prefix product (or a compensated prefix sum of
+//     log(1 - alpha)) by warp shuffles, carried across chunks;
+//   * the backward walks the chunks in reverse, carrying the suffix state, and
+//     scatters the data gradient back through the same tile with 16-byte vector REDs
+//     that cover whole vertex rows.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "quadric.cuh"
+#include "raygen.cuh"
+#include "shading.cuh"
+
+namespace qsdvr {
+
+QSDVR_ERROR_WORD_ACCESSOR(fused)
+
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kThreads = kWarpsPerBlock * kWarp;
+constexpr int kRow = 36;          // floats per staged appearance row
+constexpr uint32_t kMaxChunks = 64;  // render samples per ray <= 2048
+constexpr int kC = 32;
+
+enum Pass { kForward = 0, kBackward = 1, kTrain = 2 };
+
+struct Params {
+    const qsdvr_ray_info *rays;
+    const float *origin;
+    const float *dir;
+    uint32_t n;
+    uint32_t R;
+    float interval, k, volume_offset;
+    const void *sdf;   // [R^3][8]
+    const void *data;  // [(R+1)^3][32]
+    float *color;
+    const float *target;
+    const float *grad_color;
+    float *sdf_grad;
+    float *data_grad;
+    float *loss;
+    float grad_scale;
+};
+
+// ---- storage access --------------------------------------------------------------------
+
+__device__ __forceinline__ float bf_lo(uint32_t v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
+
+template <typename S>
+struct Store;
+
+template <>
+struct Store<float> {
+    __device__ static void cell(const void *g, uint32_t c, float *a) {
+        const float *p = static_cast<const float *>(g) + 8ull * c;
+        const float4 lo = ld4(p), hi = ld4(p + 4);
+        a[0] = lo.x; a[1] = lo.y; a[2] = lo.z; a[3] = lo.w;
+        a[4] = hi.x; a[5] = hi.y; a[6] = hi.z;
+    }
+    __device__ static float4 quad(const void *d, uint32_t v, int q) {
+        return ld4(static_cast<const float *>(d) + 32ull * v + 4 * q);
+    }
+};
+
+template <>
+struct Store<__nv_bfloat16> {
+    __device__ static void cell(const void *g, uint32_t c, float *a) {
+        const uint4 r = *reinterpret_cast<const uint4 *>(static_cast<const __nv_bfloat16 *>(g) + 8ull * c);
+        a[0] = bf_lo(r.x); a[1] = bf_hi(r.x); a[2] = bf_lo(r.y); a[3] = bf_hi(r.y);
+        a[4] = bf_lo(r.z); a[5] = bf_hi(r.z); a[6] = bf_lo(r.w);
+    }
+    __device__ static float4 quad(const void *d, uint32_t v, int q) {
+        const uint2 r = *reinterpret_cast<const uint2 *>(static_cast<const __nv_bfloat16 *>(d) + 32ull * v + 4 * q);
+        return make_float4(bf_lo(r.x), bf_hi(r.x), bf_lo(r.y), bf_hi(r.y));
+    }
+};
+
+__device__ __forceinline__ float lerp_ref(float a, float b, float x) { return a * (1 - x) + b * x; }
+__device__ __forceinline__ float4 lerp4(float4 a, float4 b, float x) {
+    return make_float4(lerp_ref(a.x, b.x, x), lerp_ref(a.y, b.y, x), lerp_ref(a.z, b.z, x), lerp_ref(a.w, b.w, x));
+}
+__device__ __forceinline__ float4 scale4(float4 v, float w) { return make_float4(v.x * w, v.y * w, v.z * w, v.w * w); }
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ bool cell_in_grid(const CellPoint &c, uint32_t R) {
+    return (unsigned)c.cx < R && (unsigned)c.cy < R && (unsigned)c.cz < R;
+}
+
+// Per-lane state of one render sample of a chunk.
+struct Sample {
+    bool valid;      // sample exists and all its cells are inside the grid
+    float alpha;
+    float e0, e1;    // exp(-k sdf_i), exp(-k sdf_{i+1})
+    f3 rgb, spec, nrm;
+    CellPoint c1;    // SDF sample i+1
+    CellPoint cr;    // render sample i
+    uint32_t vbase;  // base vertex of the trilinear fetch
+    float wx, wy, wz;
+};
+
+// Forward evaluation of render sample i = chunk*32 + lane (kernel/camera.cu:60-96,
+// kernel/surface.cu:54-115, kernel/render.cu:98-179, :239-244).  Leaves the sample's
+// interpolated 32 channels in the warp's tile.
+template <bool kCompat, typename S>
+__device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t nr, uint32_t chunk, int lane,
+                                           float *tile, Sample &s) {
+    const uint32_t R = p.R;
+    const uint32_t i = chunk * kWarp + lane;
+    const bool live = i < nr;
+    bool ok = live;
+    // SDF sample i+1 (this lane's interval end); sample i comes from the previous lane.
+    s.c1 = to_cell(march(o, d, (float)(i + 1), p.interval), p.volume_offset, R);
+    float a1[7];
+    float s1 = 0.0f;
+    if (live) {
+        if (cell_in_grid(s.c1, R)) {
+            Store<S>::cell(p.sdf, (uint32_t)s.c1.index, a1);
+            s1 = quad_sdf(a1, s.c1.u, (float)R);
+        } else {
+            ok = false;
+        }
+    }
+    float s0 = __shfl_up_sync(kFull, s1, 1);
+    if (lane == 0 && live) {
+        const CellPoint c0 = to_cell(march(o, d, (float)i, p.interval), p.volume_offset, R);
+        if (cell_in_grid(c0, R)) {
+            float a0[7];
+            Store<S>::cell(p.sdf, (uint32_t)c0.index, a0);
+            s0 = quad_sdf(a0, c0.u, (float)R);
+        } else {
+            ok = false;
+        }
+    }
+    const bool ok_prev = __shfl_up_sync(kFull, ok, 1);
+    if (lane > 0) ok = ok && ok_prev;  // sdf_i is only valid if the previous lane's cell was
+    // render sample i
+    s.cr = to_cell(midpoint(o, d, i, p.interval), p.volume_offset, R);
+    float ar[7];
+    if (live && cell_in_grid(s.cr, R)) {
+        Store<S>::cell(p.sdf, (uint32_t)s.cr.index, ar);
+        s.nrm = quad_normal(ar, s.cr.u);
+    } else {
+        ok = false;
+        s.nrm = f3{0.0f, 0.0f, 1.0f};
+    }
+    if (live && !ok) flag_error(QSDVR_DEVERR_INDEX);
+    s.valid = ok;
+    s.e0 = expf(-p.k * s0);
+    s.e1 = expf(-p.k * s1);
+    s.alpha = ok ? fmaxf((s.e1 - s.e0) / (1.0f + s.e1), 0.0f) : 0.0f;
+    // trilinear weights and base vertex (kernel/render.cu:107-111)
+    s.wx = (s.cr.u.x + 1.0f) / 2.0f;
+    s.wy = (s.cr.u.y + 1.0f) / 2.0f;
+    s.wz = (s.cr.u.z + 1.0f) / 2.0f;
+    const uint32_t R1 = R + 1;
+    s.vbase = kCompat ? (uint32_t)s.cr.index
+                      : (uint32_t)s.cr.cx + (uint32_t)s.cr.cy * R1 + (uint32_t)s.cr.cz * (R1 * R1);
+    // gather: groups of 8 lanes fetch one sample's 8 corner rows, 4 samples per step
+    const uint32_t sy = R1, sz = R1 * R1;
+    const int q = lane & 7;
+#pragma unroll 2
+    for (int st = 0; st < 8; ++st) {
+        const int j = st * 4 + (lane >> 3);
+        const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
+        const float gx = __shfl_sync(kFull, s.wx, j), gy = __shfl_sync(kFull, s.wy, j),
+                    gz = __shfl_sync(kFull, s.wz, j);
+        const bool gok = __shfl_sync(kFull, s.valid, j);
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (gok) {
+            const float4 v000 = Store<S>::quad(p.data, vb, q), v001 = Store<S>::quad(p.data, vb + 1, q);
+            const float4 v010 = Store<S>::quad(p.data, vb + sy, q), v011 = Store<S>::quad(p.data, vb + sy + 1, q);
+            const float4 v100 = Store<S>::quad(p.data, vb + sz, q), v101 = Store<S>::quad(p.data, vb + sz + 1, q);
+            const float4 v110 = Store<S>::quad(p.data, vb + sz + sy, q),
+                         v111 = Store<S>::quad(p.data, vb + sz + sy + 1, q);
+            const float4 a0 = lerp4(lerp4(v000, v001, gx), lerp4(v010, v011, gx), gy);
+            const float4 a1v = lerp4(lerp4(v100, v101, gx), lerp4(v110, v111, gx), gy);
+            v = lerp4(a0, a1v, gz);
+        }
+        st4(tile + j * kRow + 4 * q, v);
+    }
+    __syncwarp();
+    if (s.valid) {
+        float dch[kC];
+        const float *row = tile + lane * kRow;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const float4 v = ld4(row + 4 * t);
+            dch[4 * t] = v.x; dch[4 * t + 1] = v.y; dch[4 * t + 2] = v.z; dch[4 * t + 3] = v.w;
+        }
+        s.rgb = shade<kCompat>(s.nrm, d, dch, &s.spec);
+    } else {
+        s.rgb = f3{0.0f, 0.0f, 0.0f};
+        s.spec = f3{0.0f, 0.0f, 0.0f};
+    }
+}
+
+// Alpha only (no normal, gather or shading): what the backward-only pass needs to
+// rebuild the transmittance at each chunk start.  Validity matches eval_chunk.
+template <typename S>
+__device__ __forceinline__ void eval_alpha(const Params &p, f3 o, f3 d, uint32_t nr, uint32_t chunk, int lane,
+                                           Sample &s) {
+    const uint32_t R = p.R;
+    const uint32_t i = chunk * kWarp + lane;
+    const bool live = i < nr;
+    bool ok = live;
+    const CellPoint c1 = to_cell(march(o, d, (float)(i + 1), p.interval), p.volume_offset, R);
+    float s1 = 0.0f;
+    if (live) {
+        if (cell_in_grid(c1, R)) {
+            float a1[7];
+            Store<S>::cell(p.sdf, (uint32_t)c1.index, a1);
+            s1 = quad_sdf(a1, c1.u, (float)R);
+        } else {
+            ok = false;
+        }
+    }
+    float s0 = __shfl_up_sync(kFull, s1, 1);
+    if (lane == 0 && live) {
+        const CellPoint c0 = to_cell(march(o, d, (float)i, p.interval), p.volume_offset, R);
+        if (cell_in_grid(c0, R)) {
+            float a0[7];
+            Store<S>::cell(p.sdf, (uint32_t)c0.index, a0);
+            s0 = quad_sdf(a0, c0.u, (float)R);
+        } else {
+            ok = false;
+        }
+    }
+    const bool ok_prev = __shfl_up_sync(kFull, ok, 1);
+    if (lane > 0) ok = ok && ok_prev;
+    if (live && !cell_in_grid(to_cell(midpoint(o, d, i, p.interval), p.volume_offset, R), R)) ok = false;
+    s.valid = ok;
+    s.e0 = expf(-p.k * s0);
+    s.e1 = expf(-p.k * s1);
+    s.alpha = ok ? fmaxf((s.e1 - s.e0) / (1.0f + s.e1), 0.0f) : 0.0f;
+}
+
+// Transmittance at each lane's sample given the value at the chunk start.  kLogT uses the
+// compensated running sum of log(1 - alpha) (carry = sum, comp = Kahan compensation).
+template <bool kLogT>
+struct Transmittance {
+    float carry = kLogT ? 0.0f : 1.0f;
+    float comp = 0.0f;
+
+    // returns T_i for this lane and advances the carry past the chunk
+    __device__ __forceinline__ float step(float alpha, bool valid, int lane) {
+        if (kLogT) {
+            float incl = valid ? log1pf(-alpha) : 0.0f;
+#pragma unroll
+            for (int o = 1; o < kWarp; o <<= 1) {
+                const float v = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += v;
+            }
+            float excl = __shfl_up_sync(kFull, incl, 1);
+            if (lane == 0) excl = 0.0f;
+            const float T = expf(carry + excl);
+            const float tot = __shfl_sync(kFull, incl, kWarp - 1);
+            const float y = tot - comp;
+            const float t = carry + y;
+            // once alpha == 1 the sum is -inf for good: keep the compensation finite
+            comp = isfinite(t) ? (t - carry) - y : 0.0f;
+            carry = t;
+            return T;
+        } else {
+            float incl = valid ? 1.0f - alpha : 1.0f;
+#pragma unroll
+            for (int o = 1; o < kWarp; o <<= 1) {
+                const float v = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl *= v;
+            }
+            float excl = __shfl_up_sync(kFull, incl, 1);
+            if (lane == 0) excl = 1.0f;
+            const float T = carry * excl;
+            carry *= __shfl_sync(kFull, incl, kWarp - 1);
+            return T;
+        }
+    }
+};
+
+// Scatter the data-gradient tile (rows of 32 channels per lane's sample) through the
+// trilinear weights: 8 lanes per sample, one 16-byte RED per lane and corner.
+__device__ __forceinline__ void scatter_tile(const Params &p, const float *tile, const Sample &s, int lane) {
+    const uint32_t R1 = p.R + 1, sy = R1, sz = R1 * R1;
+    const int q = lane & 7;
+#pragma unroll 2
+    for (int st = 0; st < 8; ++st) {
+        const int j = st * 4 + (lane >> 3);
+        const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
+        const float px = __shfl_sync(kFull, s.wx, j), py = __shfl_sync(kFull, s.wy, j),
+                    pz = __shfl_sync(kFull, s.wz, j);
+        const bool ok = __shfl_sync(kFull, s.valid, j);
+        if (!ok) continue;
+        const float4 g = ld4(tile + j * kRow + 4 * q);
+        // kernel/render.cu:136-151
+        const float dx = 1 - px, dy = 1 - py;
+        const float4 a0 = scale4(g, 1 - pz), a1 = scale4(g, pz);
+        const float4 a00 = scale4(a0, dy), a01 = scale4(a0, py), a10 = scale4(a1, dy), a11 = scale4(a1, py);
+        float *b = p.data_grad + 32ull * vb + 4 * q;
+        red4(b, scale4(a00, dx));
+        red4(b + 32, scale4(a00, px));
+        red4(b + 32ull * sy, scale4(a01, dx));
+        red4(b + 32ull * sy + 32, scale4(a01, px));
+        red4(b + 32ull * sz, scale4(a10, dx));
+        red4(b + 32ull * sz + 32, scale4(a10, px));
+        red4(b + 32ull * (sz + sy), scale4(a11, dx));
+        red4(b + 32ull * (sz + sy) + 32, scale4(a11, px));
+    }
+}
+
+__device__ __forceinline__ void red_cell(float *g8, uint32_t cell, const float *g) {
+    float *b = g8 + 8ull * cell;
+    red4(b, make_float4(g[0], g[1], g[2], g[3]));
+    red4(b + 4, make_float4(g[4], g[5], g[6], 0.0f));
+}
+
+template <bool kCompat, typename S, int kPass, bool kLogT>
+__global__ void __launch_bounds__(kThreads) render_kernel(const Params p) {
+    __shared__ __align__(16) float tiles[kWarpsPerBlock][kWarp * kRow];
+    __shared__ float block_sq[kWarpsPerBlock];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float *tile = tiles[w];
+    const uint32_t r = blockIdx.x * kWarpsPerBlock + w;
+    float sq = 0.0f;
+    if (r < p.n) {
+        const qsdvr_ray_info info = p.rays[r];
+        const uint32_t ns = info.sdf_count;
+        const uint32_t nr = ns > 1 ? ns - 1 : 0;
+        const uint32_t chunks = (nr + kWarp - 1) / kWarp;
+        const f3 o = load3(p.origin + 3ull * r), d = load3(p.dir + 3ull * r);
+        f3 C{0.0f, 0.0f, 0.0f};
+        bool run = nr > 0;
+        if (chunks > kMaxChunks) {
+            if (lane == 0) flag_error(QSDVR_DEVERR_RAY);
+            run = false;
+        }
+        Sample s;
+        Transmittance<kLogT> tr;
+        float ts_lo = 0.0f, ts_hi = 0.0f;  // transmittance carry at the start of chunk lane / lane+32
+        // ---------------- forward
+        if (kPass != kBackward || run) {
+            if (run) {
+                f3 acc{0.0f, 0.0f, 0.0f};
+                for (uint32_t c = 0; c < chunks; ++c) {
+                    if ((c & 31) == (uint32_t)lane) {
+                        if (c < 32) ts_lo = tr.carry; else ts_hi = tr.carry;
+                    }
+                    if (kPass == kBackward) {
+                        eval_alpha<S>(p, o, d, nr, c, lane, s);
+                        tr.step(s.alpha, s.valid, lane);
+                    } else {
+                        eval_chunk<kCompat, S>(p, o, d, nr, c, lane, tile, s);
+                        const float T = tr.step(s.alpha, s.valid, lane);
+                        acc.x += s.rgb.x * s.alpha * T;
+                        acc.y += s.rgb.y * s.alpha * T;
+                        acc.z += s.rgb.z * s.alpha * T;
+                        __syncwarp();
+                    }
+                }
+                C = f3{warp_sum(acc.x), warp_sum(acc.y), warp_sum(acc.z)};
+            }
+            if (kPass != kBackward && lane == 0) store3(p.color + 3ull * r, C);
+        }
+        // ---------------- loss gradient
+        f3 g{0.0f, 0.0f, 0.0f};
+        if (kPass == kTrain) {
+            const f3 t = load3(p.target + 3ull * r);
+            const f3 e{C.x - t.x, C.y - t.y, C.z - t.z};
+            sq = e.x * e.x + e.y * e.y + e.z * e.z;
+            g = f3{p.grad_scale * e.x, p.grad_scale * e.y, p.grad_scale * e.z};
+        } else if (kPass == kBackward) {
+            g = load3(p.grad_color + 3ull * r);
+        }
+        // ---------------- backward (chunks in reverse, suffix state carried)
+        if (kPass != kForward && run) {
+            f3 suf{0.0f, 0.0f, 0.0f};  // compat: sum_{m>chunk} T a c ; fixed: R after the chunk
+            float next_this = 0.0f;    // d_this term of the first sample of the following chunk
+            for (int c = (int)chunks - 1; c >= 0; --c) {
+                const float t0 = __shfl_sync(kFull, c < 32 ? ts_lo : ts_hi, c & 31);
+                tr.carry = t0;
+                eval_chunk<kCompat, S>(p, o, d, nr, (uint32_t)c, lane, tile, s);
+                const float T = tr.step(s.alpha, s.valid, lane);
+                const float a = s.alpha;
+                const uint32_t i = (uint32_t)c * kWarp + lane;
+                float dl = 0.0f;  // dL/dalpha_i
+                if (kCompat) {
+                    // kernel/render.cu:279-313: Tac = sum over later samples of T a c
+                    f3 v = s.valid ? f3{s.rgb.x * T * a, s.rgb.y * T * a, s.rgb.z * T * a} : f3{0.0f, 0.0f, 0.0f};
+#pragma unroll
+                    for (int off = 1; off < kWarp; off <<= 1) {
+                        const float x = __shfl_down_sync(kFull, v.x, off), y = __shfl_down_sync(kFull, v.y, off),
+                                    z = __shfl_down_sync(kFull, v.z, off);
+                        if (lane + off < kWarp) {
+                            v.x += x;
+                            v.y += y;
+                            v.z += z;
+                        }
+                    }
+                    f3 after{__shfl_down_sync(kFull, v.x, 1), __shfl_down_sync(kFull, v.y, 1),
+                             __shfl_down_sync(kFull, v.z, 1)};
+                    if (lane == kWarp - 1) after = f3{0.0f, 0.0f, 0.0f};
+                    after.x += suf.x;
+                    after.y += suf.y;
+                    after.z += suf.z;
+                    if (s.valid) {
+                        const f3 dc{s.rgb.x * T + after.x / (a - 1), s.rgb.y * T + after.y / (a - 1),
+                                    s.rgb.z * T + after.z / (a - 1)};
+                        dl = g.x * dc.x + g.y * dc.y + g.z * dc.z;
+                    }
+                    suf.x += __shfl_sync(kFull, v.x, 0);
+                    suf.y += __shfl_sync(kFull, v.y, 0);
+                    suf.z += __shfl_sync(kFull, v.z, 0);
+                } else {
+                    // R_i = a_i c_i + (1 - a_i) R_{i+1}: reverse scan of affine maps, no division
+                    f3 A = s.valid ? f3{a * s.rgb.x, a * s.rgb.y, a * s.rgb.z} : f3{0.0f, 0.0f, 0.0f};
+                    float B = s.valid ? 1.0f - a : 1.0f;
+#pragma unroll
+                    for (int off = 1; off < kWarp; off <<= 1) {
+                        const float x = __shfl_down_sync(kFull, A.x, off), y = __shfl_down_sync(kFull, A.y, off),
+                                    z = __shfl_down_sync(kFull, A.z, off), b = __shfl_down_sync(kFull, B, off);
+                        if (lane + off < kWarp) {
+                            A.x += B * x;
+                            A.y += B * y;
+                            A.z += B * z;
+                            B *= b;
+                        }
+                    }
+                    const f3 Ri{A.x + B * suf.x, A.y + B * suf.y, A.z + B * suf.z};
+                    f3 Rn{__shfl_down_sync(kFull, Ri.x, 1), __shfl_down_sync(kFull, Ri.y, 1),
+                          __shfl_down_sync(kFull, Ri.z, 1)};
+                    if (lane == kWarp - 1) Rn = suf;
+                    if (s.valid) dl = T * (g.x * (s.rgb.x - Rn.x) + g.y * (s.rgb.y - Rn.y) + g.z * (s.rgb.z - Rn.z));
+                    suf = f3{__shfl_sync(kFull, Ri.x, 0), __shfl_sync(kFull, Ri.y, 0), __shfl_sync(kFull, Ri.z, 0)};
+                }
+                // dalpha/dsdf (kernel/render.cu:271-278), zero where alpha == 0
+                float d_this = 0.0f, d_next = 0.0f;
+                if (s.valid && a != 0.0f) {
+                    const float inv = 1.0f / (1.0f + s.e1);
+                    d_next = -p.k * s.e1 * (1.0f + s.e0) * inv * inv;
+                    d_this = p.k * s.e0 * inv;
+                }
+                const float mine_this = dl * d_this;
+                float from_next = __shfl_down_sync(kFull, mine_this, 1);
+                if (lane == kWarp - 1) from_next = next_this;
+                next_this = __shfl_sync(kFull, mine_this, 0);
+                if (s.valid) {
+                    // SDF sample i+1 and, for the ray's first lane, SDF sample 0
+                    const float gs1 = dl * d_next + (i + 1 < nr ? from_next : 0.0f);
+                    float a1[7], gq[7];
+                    Store<S>::cell(p.sdf, (uint32_t)s.c1.index, a1);
+                    quad_sdf_grad(a1, s.c1.u, (float)p.R, gs1, gq);
+                    // rgb gradient -> shader backward (data gradient into the tile, normal gradient)
+                    const f3 grgb{g.x * T * a, g.y * T * a, g.z * T * a};
+                    float dch[kC], gd[kC];
+                    float *row = tile + lane * kRow;
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const float4 v = ld4(row + 4 * t);
+                        dch[4 * t] = v.x; dch[4 * t + 1] = v.y; dch[4 * t + 2] = v.z; dch[4 * t + 3] = v.w;
+                    }
+                    const f3 gn = shade_backward<kCompat>(grgb, s.nrm, d, dch, s.spec, gd);
+#pragma unroll
+                    for (int t = 0; t < 8; ++t)
+                        st4(row + 4 * t, make_float4(gd[4 * t], gd[4 * t + 1], gd[4 * t + 2], gd[4 * t + 3]));
+                    float ar[7], gr[6];
+                    Store<S>::cell(p.sdf, (uint32_t)s.cr.index, ar);
+                    quad_normal_grad(ar, s.cr.u, gn, gr);
+                    if (s.cr.index == s.c1.index) {
+#pragma unroll
+                        for (int t = 0; t < 6; ++t) gq[t] += gr[t];
+                        red_cell(p.sdf_grad, (uint32_t)s.c1.index, gq);
+                    } else {
+                        red_cell(p.sdf_grad, (uint32_t)s.c1.index, gq);
+                        const float g7[7] = {gr[0], gr[1], gr[2], gr[3], gr[4], gr[5], 0.0f};
+                        red_cell(p.sdf_grad, (uint32_t)s.cr.index, g7);
+                    }
+                    if (i == 0) {
+                        const CellPoint c0 = to_cell(march(o, d, 0.0f, p.interval), p.volume_offset, p.R);
+                        float a0[7], g0[7];
+                        Store<S>::cell(p.sdf, (uint32_t)c0.index, a0);
+                        quad_sdf_grad(a0, c0.u, (float)p.R, mine_this, g0);
+                        red_cell(p.sdf_grad, (uint32_t)c0.index, g0);
+                    }
+                }
+                __syncwarp();
+                scatter_tile(p, tile, s, lane);
+                __syncwarp();
+            }
+        }
+    }
+    if (kPass == kTrain) {
+        sq = warp_sum(sq);
+        if (lane == 0) block_sq[w] = sq;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float t = 0.0f;
+            for (int k = 0; k < kWarpsPerBlock; ++k) t += block_sq[k];
+            atomicAdd(p.loss, t);
+        }
+    }
+}
+
+template <int kPass>
+int launch(const qsdvr_render_args *a, cudaStream_t stream) {
+    Params p;
+    p.rays = a->rays;
+    p.origin = a->origin;
+    p.dir = a->dir;
+    p.n = a->ray_count;
+    p.R = a->reso;
+    p.interval = a->interval;
+    p.k = a->logistic_coef;
+    p.volume_offset = (float)a->reso / 2.0f;
+    p.sdf = a->sdf_grid;
+    p.data = a->data;
+    p.color = a->color;
+    p.target = a->target;
+    p.grad_color = a->grad_color;
+    p.sdf_grad = a->sdf_grad;
+    p.data_grad = a->data_grad;
+    p.loss = a->loss;
+    p.grad_scale = a->grad_scale;
+    const unsigned blocks = grid_for(a->ray_count, kWarpsPerBlock);
+    const bool compat = a->mode == QSDVR_MODE_COMPAT;
+    const bool bf16 = a->storage == QSDVR_STORAGE_BF16;
+    const bool logt = a->transmittance == QSDVR_TRANSMITTANCE_LOG;
+#define QSDVR_LAUNCH(C, S, L) render_kernel<C, S, kPass, L><<<blocks, kThreads, 0, stream>>>(p)
+    if (compat) {
+        if (bf16) { if (logt) QSDVR_LAUNCH(true, __nv_bfloat16, true); else QSDVR_LAUNCH(true, __nv_bfloat16, false); }
+        else { if (logt) QSDVR_LAUNCH(true, float, true); else QSDVR_LAUNCH(true, float, false); }
+    } else {
+        if (bf16) { if (logt) QSDVR_LAUNCH(false, __nv_bfloat16, true); else QSDVR_LAUNCH(false, __nv_bfloat16, false); }
+        else { if (logt) QSDVR_LAUNCH(false, float, true); else QSDVR_LAUNCH(false, float, false); }
+    }
+#undef QSDVR_LAUNCH
+    return check_launch(kPass == kForward ? "qsdvr_render_forward"
+                                          : (kPass == kBackward ? "qsdvr_render_backward" : "qsdvr_render_train"));
+}
+
+int validate(const qsdvr_render_args *a, int pass) {
+    if (!a) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null args");
+    if (a->ray_count && (!a->rays || !a->origin || !a->dir || !a->sdf_grid || !a->data))
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null ray or grid pointer");
+    if (a->reso == 0 || a->reso > 1290)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: reso %u out of range", a->reso);
+    if (a->mode != QSDVR_MODE_COMPAT && a->mode != QSDVR_MODE_FIXED)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: bad mode %d", a->mode);
+    if (a->storage != QSDVR_STORAGE_F32 && a->storage != QSDVR_STORAGE_BF16)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: bad storage %d", a->storage);
+    if (a->transmittance != QSDVR_TRANSMITTANCE_PRODUCT && a->transmittance != QSDVR_TRANSMITTANCE_LOG)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: bad transmittance form %d", a->transmittance);
+    if (!(a->interval > 0.0f)) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: interval must be > 0");
+    if (!aligned(a->sdf_grid, 16) || !aligned(a->data, 16) || !aligned(a->rays, 16))
+        return set_error(QSDVR_ERR_ALIGNMENT, "render: rays, sdf_grid and data need 16-byte alignment");
+    if (pass != kForward && a->ray_count &&
+        (!a->sdf_grad || !a->data_grad || !aligned(a->sdf_grad, 16) || !aligned(a->data_grad, 16)))
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: gradient buffers missing or not 16-byte aligned");
+    if (pass != kBackward && a->ray_count && !a->color)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null color output");
+    if (pass == kBackward && a->ray_count && !a->grad_color)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null grad_color");
+    if (pass == kTrain && a->ray_count && (!a->target || !a->loss))
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null target or loss");
+    return QSDVR_OK;
+}
+
+}  // namespace
+}  // namespace qsdvr
+
+using namespace qsdvr;
+
+extern "C" int qsdvr_render_forward(const qsdvr_render_args *args, cudaStream_t stream) {
+    const int st = validate(args, kForward);
+    if (st != QSDVR_OK || args->ray_count == 0) return st;
+    return launch<kForward>(args, stream);
+}
+
+extern "C" int qsdvr_render_backward(const qsdvr_render_args *args, cudaStream_t stream) {
+    const int st = validate(args, kBackward);
+    if (st != QSDVR_OK || args->ray_count == 0) return st;
+    return launch<kBackward>(args, stream);
+}
+
+extern "C" int qsdvr_render_train(const qsdvr_render_args *args, cudaStream_t stream) {
+    const int st = validate(args, kTrain);
+    if (st != QSDVR_OK || args->ray_count == 0) return st;
+    return launch<kTrain>(args, stream);
+}

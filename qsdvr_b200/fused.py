@@ -1,0 +1,232 @@
+"""Fused render path: one kernel per pass over a batch of rays (include/qsdvr_b200.h,
+qsdvr_render_*).
+
+* ``render_forward`` / ``render_backward`` / ``render_train`` call the C ABI directly;
+* ``FusedRender`` is the ``autograd.Function`` whose backward recomputes every sample
+  (memory O(rays): nothing per-sample is saved between forward and backward);
+* ``DenseRenderGrid`` is a RenderGrid (models/render.py:209-237) whose SDF is a dense
+  quadric grid [R^3][8] instead of separable layers, rendered by the fused kernels.
+
+Ray batches are the reference's per-ray tables: ``rays`` int32 [N,4] (RayInfo),
+``origin`` and ``dir`` float32 [N,3] (RayCut output after masking).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+from torch import autograd, nn
+
+from . import _lib
+from ._lib import F32, I32, P, U32, call
+
+STORAGE = {"f32": 0, "bf16": 1}
+TRANSMITTANCE = {"product": 0, "log": 1}
+MODES = {"compat": _lib.MODE_COMPAT, "fixed": _lib.MODE_FIXED}
+
+
+class RenderArgs(ctypes.Structure):
+    """qsdvr_render_args (include/qsdvr_b200.h)."""
+    _fields_ = [("rays", P), ("origin", P), ("dir", P), ("ray_count", U32), ("reso", U32), ("interval", F32),
+                ("logistic_coef", F32), ("mode", I32), ("storage", I32), ("transmittance", I32), ("reserved", I32),
+                ("sdf_grid", P), ("data", P), ("color", P), ("target", P), ("grad_color", P), ("sdf_grad", P),
+                ("data_grad", P), ("loss", P), ("grad_scale", F32)]
+
+
+_lib.extra_signatures({
+    "qsdvr_render_forward": [ctypes.POINTER(RenderArgs), P],
+    "qsdvr_render_backward": [ctypes.POINTER(RenderArgs), P],
+    "qsdvr_render_train": [ctypes.POINTER(RenderArgs), P],
+})
+
+
+def _ptr(t):
+    return t.data_ptr() if t is not None and t.numel() else None
+
+
+def _check_batch(rays, origin, direction):
+    dev = rays.device
+    if not rays.is_cuda or rays.dtype != torch.int32 or rays.dim() != 2 or rays.shape[1] != 4:
+        raise ValueError("rays must be a CUDA int32 [N,4] tensor")
+    n = rays.shape[0]
+    for t, nm in ((origin, "origin"), (direction, "dir")):
+        if t.device != dev or t.dtype != torch.float32 or t.numel() != 3 * n or not t.is_contiguous():
+            raise ValueError(f"{nm} must be a contiguous float32 [N,3] tensor on {dev}")
+    if not rays.is_contiguous():
+        raise ValueError("rays must be contiguous")
+    return dev, n
+
+
+def _grid_storage(sdf_grid, data, R):
+    if sdf_grid.dtype != data.dtype or sdf_grid.dtype not in (torch.float32, torch.bfloat16):
+        raise TypeError("sdf_grid and data must both be float32 or both bfloat16")
+    if sdf_grid.numel() != 8 * R ** 3 or data.numel() != 32 * (R + 1) ** 3:
+        raise ValueError(f"sdf_grid must be [R^3,8] and data [(R+1)^3,32] for R={R}")
+    if not (sdf_grid.is_contiguous() and data.is_contiguous()):
+        raise ValueError("grids must be contiguous")
+    return STORAGE["bf16" if sdf_grid.dtype == torch.bfloat16 else "f32"]
+
+
+def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat", transmittance="product",
+              color=None, target=None, grad_color=None, sdf_grad=None, data_grad=None, loss=None,
+              grad_scale=0.0) -> RenderArgs:
+    dev, n = _check_batch(rays, origin, direction)
+    a = RenderArgs()
+    a.rays, a.origin, a.dir = _ptr(rays), _ptr(origin), _ptr(direction)
+    a.ray_count, a.reso = n, int(reso)
+    a.interval, a.logistic_coef = float(interval), float(k)
+    a.mode = MODES[mode]
+    a.storage = _grid_storage(sdf_grid, data, int(reso))
+    a.transmittance = TRANSMITTANCE[transmittance]
+    a.sdf_grid, a.data = _ptr(sdf_grid), _ptr(data)
+    a.color, a.target, a.grad_color = _ptr(color), _ptr(target), _ptr(grad_color)
+    a.sdf_grad, a.data_grad, a.loss = _ptr(sdf_grad), _ptr(data_grad), _ptr(loss)
+    a.grad_scale = float(grad_scale)
+    return a
+
+
+def _stream(dev):
+    return ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+
+def render_forward(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat",
+                   transmittance="product", color=None):
+    """Colour of every ray [N,3]."""
+    dev, n = _check_batch(rays, origin, direction)
+    if color is None:
+        color = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color)
+    with torch.cuda.device(dev):
+        call("qsdvr_render_forward", ctypes.byref(a), _stream(dev))
+    return color
+
+
+def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
+                    mode="compat", transmittance="product"):
+    """Accumulate dL/d(sdf_grid) and dL/d(data) (fp32) for a given dL/dcolor."""
+    dev, n = _check_batch(rays, origin, direction)
+    for t, nm, shape in ((sdf_grad, "sdf_grad", sdf_grid.numel()), (data_grad, "data_grad", data.numel())):
+        if t.dtype != torch.float32 or t.numel() != shape or t.device != dev or not t.is_contiguous():
+            raise ValueError(f"{nm} must be a contiguous float32 tensor shaped like its grid")
+    g = grad_color.contiguous().float()
+    a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, grad_color=g,
+                  sdf_grad=sdf_grad, data_grad=data_grad)
+    with torch.cuda.device(dev):
+        call("qsdvr_render_backward", ctypes.byref(a), _stream(dev))
+
+
+def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
+                 mode="compat", transmittance="product", loss=None, color=None):
+    """Forward + MSE (mean over N x 3) + backward in one launch.  Returns (color, loss_sum)
+    where loss_sum accumulates sum |color - target|^2 (divide by 3N for the mean)."""
+    dev, n = _check_batch(rays, origin, direction)
+    if color is None:
+        color = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    if loss is None:
+        loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color,
+                  target=target.contiguous(), sdf_grad=sdf_grad, data_grad=data_grad, loss=loss,
+                  grad_scale=2.0 / (3.0 * max(n, 1)))
+    with torch.cuda.device(dev):
+        call("qsdvr_render_train", ctypes.byref(a), _stream(dev))
+    return color, loss
+
+
+class FusedRender(autograd.Function):
+    """Differentiable fused render.  Forward saves only its inputs; backward recomputes
+    each sample's alpha, transmittance and colour (memory O(rays))."""
+
+    @staticmethod
+    def forward(ctx, sdf_grid, data, rays, origin, direction, reso, interval, k, mode, transmittance):
+        color = render_forward(rays, origin, direction, sdf_grid.detach(), data.detach(), reso, interval, k, mode,
+                               transmittance)
+        ctx.save_for_backward(sdf_grid, data, rays, origin, direction)
+        ctx.cfg = (reso, interval, k, mode, transmittance)
+        return color
+
+    @staticmethod
+    def backward(ctx, grad_color):
+        sdf_grid, data, rays, origin, direction = ctx.saved_tensors
+        reso, interval, k, mode, transmittance = ctx.cfg
+        sg = torch.zeros(sdf_grid.shape, dtype=torch.float32, device=sdf_grid.device)
+        dg = torch.zeros(data.shape, dtype=torch.float32, device=data.device)
+        render_backward(grad_color, rays, origin, direction, sdf_grid.detach(), data.detach(), reso, interval, k, sg,
+                        dg, mode, transmittance)
+        return sg.to(sdf_grid.dtype), dg.to(data.dtype), None, None, None, None, None, None, None, None
+
+
+def pad_grid7(grid7: torch.Tensor) -> torch.Tensor:
+    """[R^3,7] (reference layout) -> [R^3,8] (16-byte-aligned rows, a7 = 0)."""
+    g = grid7.reshape(-1, 7)
+    out = torch.zeros((g.shape[0], 8), dtype=g.dtype, device=g.device)
+    out[:, :7] = g
+    return out
+
+
+class DenseRenderGrid(nn.Module):
+    """RenderGrid with a dense quadric SDF grid, rendered by the fused kernels.
+
+    Parameters are fp32 masters; with ``storage='bf16'`` the kernels read bf16 copies
+    refreshed by ``sync_storage()`` (call it after each optimizer step)."""
+
+    def __init__(self, reso: int = 128, logisticCoef: float = 5.0, interval: float = 4.0 / 256, mode: str = "compat",
+                 storage: str = "f32", transmittance: str | None = None, device="cuda", sdf_grid=None, data=None):
+        super().__init__()
+        self.reso, self.interval, self.mode, self.storage = reso, interval, mode, storage
+        self.logisticCoef = logisticCoef
+        self.transmittance = transmittance or ("log" if storage == "bf16" else "product")
+        if sdf_grid is None:
+            from .scenes import sphere_grid
+
+            sdf_grid = sphere_grid(reso, 0.5, 0.0, device=device)
+        if data is None:
+            data = torch.zeros(((reso + 1) ** 3, 32), dtype=torch.float32, device=device)
+            data[:, 31] = 1
+            data[:, 30] = 0.1
+            data[:, 27:30] = 1
+            data[:, 0:3] = 0.5
+        g = sdf_grid.reshape(-1, sdf_grid.shape[-1])
+        self.sdfGrid = nn.Parameter(pad_grid7(g) if g.shape[1] == 7 else g.contiguous().clone())
+        self.renderData = nn.Parameter(data.reshape(-1, 32).contiguous().clone())
+        self._copies = None
+        self.sync_storage()
+
+    def sync_storage(self):
+        if self.storage == "bf16":
+            self._copies = (self.sdfGrid.detach().to(torch.bfloat16), self.renderData.detach().to(torch.bfloat16))
+
+    def grids(self):
+        if self.storage == "bf16":
+            return self._copies
+        return self.sdfGrid, self.renderData
+
+    def forward(self, rays, origin, direction):
+        if self.storage == "bf16":
+            return _Bf16Render.apply(self.sdfGrid, self.renderData, self._copies[0], self._copies[1], rays, origin,
+                                     direction, self)
+        return FusedRender.apply(self.sdfGrid, self.renderData, rays, origin, direction, self.reso, self.interval,
+                                 self.logisticCoef, self.mode, self.transmittance)
+
+    def set_logisticCoef(self, logisticCoef):
+        self.logisticCoef = logisticCoef
+
+
+class _Bf16Render(autograd.Function):
+    """Forward/backward on the bf16 copies; gradients (fp32) flow to the fp32 masters."""
+
+    @staticmethod
+    def forward(ctx, sdf_master, data_master, sdf_bf16, data_bf16, rays, origin, direction, model):
+        ctx.save_for_backward(sdf_bf16, data_bf16, rays, origin, direction)
+        ctx.model = model
+        return render_forward(rays, origin, direction, sdf_bf16, data_bf16, model.reso, model.interval,
+                              model.logisticCoef, model.mode, model.transmittance)
+
+    @staticmethod
+    def backward(ctx, grad_color):
+        sdf_bf16, data_bf16, rays, origin, direction = ctx.saved_tensors
+        m = ctx.model
+        sg = torch.zeros(sdf_bf16.shape, dtype=torch.float32, device=sdf_bf16.device)
+        dg = torch.zeros(data_bf16.shape, dtype=torch.float32, device=data_bf16.device)
+        render_backward(grad_color, rays, origin, direction, sdf_bf16, data_bf16, m.reso, m.interval, m.logisticCoef,
+                        sg, dg, m.mode, m.transmittance)
+        return sg, dg, None, None, None, None, None, None

@@ -1,0 +1,194 @@
+"""GPU parity of the fused render kernels (qsdvr_render_forward / _backward / _train).
+
+compat mode is checked against the reference itself (golden pipeline + live build):
+image within 1e-5 absolute, gradients within 1e-4 relative (max-abs error over max-abs
+value).  fixed mode and BF16 storage are checked against the float64 oracle, whose
+gradients are torch autograd."""
+import numpy as np
+import pytest
+import torch
+
+import oracle.oracle as O
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+IMG_TOL = 1e-5
+GRAD_TOL = 1e-4
+
+
+def _t(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+@pytest.fixture(scope="module")
+def fz():
+    from qsdvr_b200 import _lib, fused
+
+    _lib.lib()
+    return fused
+
+
+def camera_batch(pos, size, focal, interval, R, mask=None):
+    """Rays of one camera through the drop-in RayCut (bit-exact with the reference)."""
+    from qsdvr_b200 import scenes
+    from qsdvr_b200.camera import Camera
+
+    args = scenes.look_at(pos, size, size, focal, 2.0, 6.0)
+    cam = Camera(args, interval, R)
+    cam.GenerateRayPoints(torch.ones(size * size, dtype=torch.bool) if mask is None else mask)
+    return cam
+
+
+def oracle_inputs(cam):
+    d = cam.GetRayPoints()
+    inp = {k: v.cpu() for k, v in d.items() if k != "rayList"}
+    inp["rayList"] = d["rayList"].cpu().long()
+    return inp
+
+
+def oracle_render(grid8, data, cam, R, k, compat, target=None):
+    """float64 oracle image and (if target) MSE gradients w.r.t. the grids."""
+    g7 = grid8[:, :7].double().cpu().requires_grad_()
+    dd = data.double().cpu().requires_grad_()
+    img = O.render(g7, dd, oracle_inputs(cam), k, compat)
+    if target is None:
+        return img.detach(), None, None
+    loss = ((img - target.double().cpu()) ** 2).mean()
+    gg, gd = torch.autograd.grad(loss, (g7, dd))
+    return img.detach(), gg, gd
+
+
+def test_fused_compat_vs_golden_pipeline(fz, golden_pipeline):
+    g = golden_pipeline
+    R, k, interval = g["params"]
+    R = int(R)
+    rays, origin, direction = _t(g["in_rays"]), _t(g["in_origin"]), _t(g["in_dir"])
+    grid8 = fz.pad_grid7(_t(g["grid7"]))
+    data = _t(g["data"])
+    target = _t(g["target"])
+    img = fz.render_forward(rays, origin, direction, grid8, data, R, interval, k)
+    assert np.abs(img.cpu().numpy() - g["image"]).max() < IMG_TOL
+    sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+    fz.render_backward((2.0 / img.numel()) * (img - target), rays, origin, direction, grid8, data, R, interval, k, sg,
+                       dg)
+    assert rel_err(sg[:, :7].cpu(), g["grid7_grad"]) < GRAD_TOL
+    assert rel_err(dg.cpu(), g["data_grad"]) < GRAD_TOL
+    assert float(sg[:, 7].abs().max()) == 0.0
+    # the one-launch training step gives the same colour, gradients and loss
+    sg2, dg2 = torch.zeros_like(grid8), torch.zeros_like(data)
+    col, loss = fz.render_train(target, rays, origin, direction, grid8, data, R, interval, k, sg2, dg2)
+    assert (col - img).abs().max().item() < 1e-6  # another instantiation: FMA contraction may differ
+    assert rel_err(sg2.cpu(), sg.cpu()) < 1e-6 and rel_err(dg2.cpu(), dg.cpu()) < 1e-6
+    assert abs(loss.item() - ((img - target) ** 2).sum().item()) < 1e-4 * max(1.0, loss.item())
+
+
+def test_fused_compat_vs_reference_live(fz):
+    from oracle.build_ref import load_reference
+    from qsdvr_b200 import scenes
+    from tests.golden.make_golden import reference_render
+
+    ref = load_reference()
+    if ref is None:
+        pytest.skip("reference build absent")
+    R, k, interval = 64, 10.0, 4.0 / 256  # up to ~220 samples per ray: 7 chunks
+    cam = camera_batch((0.3, -4.0, 0.4), 100, 138.9, interval, R)
+    inp = cam.GetRayPoints()
+    grid7 = scenes.sphere_grid(R, 0.5, 0.01, seed=1).reshape(-1, 7).to(DEV)
+    data = scenes.appearance(R, seed=1).to(DEV)
+    target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(2)).to(DEV)
+    want_img, want_g7, want_data = reference_render(ref, grid7, data, inp, R, k, target)
+    grid8 = fz.pad_grid7(grid7)
+    sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+    img, _ = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k, sg, dg)
+    assert (img - want_img).abs().max().item() < IMG_TOL
+    assert rel_err(sg[:, :7].cpu(), want_g7.cpu()) < GRAD_TOL
+    assert rel_err(dg.cpu(), want_data.cpu()) < GRAD_TOL
+
+
+@pytest.mark.parametrize("interval", [4.0 / 64, 4.0 / 192])
+def test_fused_fixed_vs_oracle(fz, interval):
+    from qsdvr_b200 import scenes
+
+    R, k = 24, 8.0
+    cam = camera_batch((2.2, -3.0, 1.5), 40, 55.0, interval, R)
+    grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.55, 0.01, seed=3).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=3).to(DEV)
+    target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(4)).to(DEV)
+    sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+    img, _ = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k, sg, dg,
+                             mode="fixed")
+    want, wg, wd = oracle_render(grid8, data, cam, R, k, compat=False, target=target)
+    assert (img.cpu().double() - want).abs().max().item() < IMG_TOL
+    assert rel_err(sg[:, :7].cpu(), wg) < GRAD_TOL
+    assert rel_err(dg.cpu(), wd) < GRAD_TOL
+
+
+def test_fused_bf16_storage_vs_oracle(fz):
+    """BF16 grids, FP32 arithmetic, compensated log-transmittance: compared with the
+    float64 oracle evaluated on the same bf16-rounded grids."""
+    from qsdvr_b200 import scenes
+
+    R, k, interval = 32, 10.0, 4.0 / 128
+    cam = camera_batch((-2.5, -2.9, 1.2), 48, 66.0, interval, R)
+    grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.5, 0.01, seed=5).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=5).to(DEV)
+    g16, d16 = grid8.to(torch.bfloat16), data.to(torch.bfloat16)
+    target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(6)).to(DEV)
+    for mode in ("compat", "fixed"):
+        sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+        img, _ = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, g16, d16, R, interval, k, sg, dg,
+                                 mode=mode, transmittance="log")
+        want, wg, wd = oracle_render(g16.float(), d16.float(), cam, R, k, compat=(mode == "compat"), target=target)
+        assert (img.cpu().double() - want).abs().max().item() < IMG_TOL
+        assert rel_err(sg[:, :7].cpu(), wg) < GRAD_TOL
+        assert rel_err(dg.cpu(), wd) < GRAD_TOL
+
+
+def test_log_transmittance_matches_product(fz):
+    from qsdvr_b200 import scenes
+
+    R, k, interval = 48, 20.0, 4.0 / 256
+    cam = camera_batch((0.1, 3.9, -0.8), 64, 90.0, interval, R)
+    grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.6, 0.01, seed=7).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=7).to(DEV)
+    a = fz.render_forward(cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k, "fixed", "product")
+    b = fz.render_forward(cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k, "fixed", "log")
+    assert (a - b).abs().max().item() < IMG_TOL
+
+
+def test_autograd_function_matches_train_kernel(fz):
+    from qsdvr_b200 import scenes
+
+    R, k, interval = 32, 6.0, 4.0 / 96
+    cam = camera_batch((1.5, -3.4, 1.0), 50, 70.0, interval, R)
+    model = fz.DenseRenderGrid(R, k, interval, mode="fixed", sdf_grid=scenes.sphere_grid(R, 0.5, 0.01, device=DEV),
+                               data=scenes.appearance(R, device=DEV))
+    target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(8)).to(DEV)
+    img = model(cam.rayList, cam.originList, cam.dirList)
+    loss = ((img - target) ** 2).mean()
+    loss.backward()
+    sg, dg = torch.zeros_like(model.sdfGrid), torch.zeros_like(model.renderData)
+    col, ls = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, model.sdfGrid.detach(),
+                              model.renderData.detach(), R, interval, k, sg, dg, mode="fixed")
+    assert (col - img.detach()).abs().max().item() < 1e-6
+    assert abs(ls.item() / (3 * col.shape[0]) - loss.item()) < 1e-6
+    assert rel_err(model.sdfGrid.grad.cpu(), sg.cpu()) < 1e-6
+    assert rel_err(model.renderData.grad.cpu(), dg.cpu()) < 1e-6
+
+
+def test_rays_outside_grid_are_flagged_not_faulting(fz):
+    from qsdvr_b200 import _lib
+
+    R = 8
+    _lib.device_error()
+    rays = torch.tensor([[10, 0, 9, 0], [0, 10, 0, 9], [5, 10, 4, 9]], dtype=torch.int32, device=DEV)
+    origin = torch.tensor([[0.0, 0.0, 0.0], [0.0, 0.0, 0.0], [3.0, 0.0, 0.0]], device=DEV)  # third starts outside
+    direction = torch.tensor([[1.0, 0.0, 0.0], [1.0, 0.0, 0.0], [1.0, 0.0, 0.0]], device=DEV)
+    grid8 = torch.zeros((R ** 3, 8), device=DEV)
+    grid8[:, 3] = 1.0
+    data = torch.ones(((R + 1) ** 3, 32), device=DEV)
+    img = fz.render_forward(rays, origin, direction, grid8, data, R, 0.05, 5.0)
+    assert torch.isfinite(img).all()
+    assert img[2].abs().max().item() == 0.0
+    assert _lib.device_error() & _lib.DEVERR_INDEX
