@@ -55,7 +55,7 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 20 ms during the timed region."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -69,7 +69,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                          "--format=csv,noheader,nounits", "-lms", "20"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -187,11 +187,13 @@ def time_device(step, steps, warmup, stream):
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")
     start.record(stream)
     for i in range(steps):
         step(i, ev[i])
     stop.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     total_ms = start.elapsed_time(stop)
     kern_ms = [a.elapsed_time(b) for a, b in ev]
     return total_ms, kern_ms
@@ -249,8 +251,12 @@ def run_ours(args, cfg, device, ws, rank):
         sg.zero_()
         dg.zero_()
         loss.zero_()
+        if ev is not None:
+            ev[0].record(stream)
         fused.render_train(dev_in["target"], dev_in["rays"], dev_in["origin"], dev_in["dir"], sdf_k, data_k, R,
                            cfg["interval"], K_LOGISTIC, sg, dg, "compat", transmittance, loss=loss, color=color)
+        if ev is not None:
+            ev[1].record(stream)
         loss_host.copy_(loss, non_blocking=True)
 
     if ws > 1:
@@ -388,7 +394,7 @@ def run_reference(args, cfg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plain256", choices=sorted(WORKLOADS))

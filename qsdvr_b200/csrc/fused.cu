@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(kThreads) render_kernel(const Params p) {
         if (kPass == kTrain) {
             const f3 t = load3(p.target + 3ull * r);
             const f3 e{C.x - t.x, C.y - t.y, C.z - t.z};
-            sq = e.x * e.x + e.y * e.y + e.z * e.z;
+            if (lane == 0) sq = e.x * e.x + e.y * e.y + e.z * e.z;  // C is warp-uniform: count it once
             g = f3{p.grad_scale * e.x, p.grad_scale * e.y, p.grad_scale * e.z};
         } else if (kPass == kBackward) {
             g = load3(p.grad_color + 3ull * r);
