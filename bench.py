@@ -400,10 +400,13 @@ def main():
     ap.add_argument("--workload", default="plain256", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-rays", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--views", type=int, default=None, help="override the number of camera views (ray pool size)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    cfg = WORKLOADS[args.workload]
+    cfg = dict(WORKLOADS[args.workload])
+    if args.views:
+        cfg["views"] = args.views
     ws, rank, local = dist_env()
     if args.impl == "reference":
         if rank == 0:
