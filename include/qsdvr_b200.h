@@ -87,6 +87,21 @@ int qsdvr_ray_cut(const qsdvr_camera *camera, const uint8_t *mask, qsdvr_ray_inf
                   float *dir, float interval, uint32_t pixel_count, uint32_t *totals, void *workspace,
                   size_t workspace_bytes, cudaStream_t stream);
 
+/* Largest pixel_count qsdvr_ray_cut_noalloc accepts (2048 x 2048). */
+#define QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS 4194304u
+
+/* RayCut for callers that cannot allocate device memory (an application whose device
+ * memory is all owned by its own pool, or a host that gives a plugin nothing but its input
+ * and output buffers).  No counterpart in the reference.  Same arguments and results as
+ * qsdvr_ray_cut minus the workspace; the scan's scratch is a fixed 128 KiB array in the
+ * library's device image, held on every GPU that loads the library until the process
+ * exits.  Rejects pixel_count > QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress) with the device
+ * current; make that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other streams, other host threads) race. */
+int qsdvr_ray_cut_noalloc(const qsdvr_camera *camera, const uint8_t *mask, qsdvr_ray_info *rays, float *origin,
+                          float *dir, float interval, uint32_t pixel_count, uint32_t *totals, cudaStream_t stream);
+
 /* Replaces GenerateRayPoints (kernel/camera.cu:132-147, include/camera.h:59).
  * sdf_capacity / render_capacity are the lengths of the sample lists. */
 int qsdvr_generate_ray_points(const qsdvr_ray_info *rays, const float *origin, const float *dir,

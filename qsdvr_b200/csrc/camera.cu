@@ -263,3 +263,73 @@ extern "C" int qsdvr_generate_ray_points(const qsdvr_ray_info *rays, const float
         render_points, render_index, view_dir, sdf_capacity, render_capacity);
     return check_launch("qsdvr_generate_ray_points");
 }
+
+// ---- RayCut without any allocation -------------------------------------------------------
+// Some callers cannot allocate device memory at all: an application whose device memory is
+// owned up front by its own pool or arena (a cudaMalloc would fail or fragment it), or a host
+// that hands a plugin only the buffers of its inputs and outputs.  Such a caller has no way to
+// provide the workspace qsdvr_ray_cut asks for, so this variant keeps the scan's per-block
+// sums in a fixed array in the library's device image instead.  Every GPU that loads the
+// library holds the array (128 KiB) until the process exits.
+namespace {
+
+constexpr uint32_t kStaticScanBlocks = QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS / kScanBlock;
+static_assert(QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS % kScanBlock == 0, "limit must be whole scan blocks");
+constexpr int kMaxDevices = 64;
+
+// One slot per scan block.  Every call overwrites each slot it uses before reading it, so no
+// slot has to start at zero; calls that overlap on the GPU share the array and race.
+static __device__ __align__(256) uint2 g_ray_cut_scratch[kStaticScanBlocks];
+
+// Device address of g_ray_cut_scratch per device.  In host code the symbol name is only a
+// host-side stand-in, so the address is looked up once per device, with that device current.
+uint2 *g_scratch_address[kMaxDevices] = {};
+
+int scratch_address(uint2 **out) {
+    int dev = 0;
+    int st = check_cuda(cudaGetDevice(&dev), "qsdvr_ray_cut_noalloc: cudaGetDevice");
+    if (st != QSDVR_OK) return st;
+    if (dev < 0 || dev >= kMaxDevices)
+        return set_error(QSDVR_ERR_UNSUPPORTED, "qsdvr_ray_cut_noalloc: device %d beyond %d", dev, kMaxDevices);
+    uint2 *p = __atomic_load_n(&g_scratch_address[dev], __ATOMIC_ACQUIRE);
+    if (p == nullptr) {
+        void *addr = nullptr;
+        st = check_cuda(cudaGetSymbolAddress(&addr, g_ray_cut_scratch), "qsdvr_ray_cut_noalloc: cudaGetSymbolAddress");
+        if (st != QSDVR_OK) return st;
+        p = static_cast<uint2 *>(addr);
+        __atomic_store_n(&g_scratch_address[dev], p, __ATOMIC_RELEASE);
+    }
+    *out = p;
+    return QSDVR_OK;
+}
+
+}  // namespace
+
+extern "C" int qsdvr_ray_cut_noalloc(const qsdvr_camera *camera, const uint8_t *mask, qsdvr_ray_info *rays,
+                                     float *origin, float *dir, float interval, uint32_t pixel_count, uint32_t *totals,
+                                     cudaStream_t stream) {
+    if (!camera || !mask || !rays || !origin || !dir || !totals)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_cut_noalloc: null pointer");
+    if (pixel_count > QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT,
+                         "qsdvr_ray_cut_noalloc: pixel_count %u exceeds the fixed scratch limit of %u pixels; "
+                         "use qsdvr_ray_cut with a caller workspace",
+                         pixel_count, (unsigned)QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS);
+    if (camera->width == 0 || (uint64_t)camera->width * camera->height < pixel_count)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_cut_noalloc: pixel_count %u exceeds %u x %u",
+                         pixel_count, camera->width, camera->height);
+    if (!(interval > 0.0f))
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_cut_noalloc: interval must be > 0");
+    if (!aligned(rays, 16))
+        return set_error(QSDVR_ERR_ALIGNMENT, "qsdvr_ray_cut_noalloc: rays need 16-byte alignment");
+    uint2 *sums = nullptr;
+    int st = scratch_address(&sums);
+    if (st != QSDVR_OK) return st;
+    if (pixel_count == 0)
+        return check_cuda(cudaMemsetAsync(totals, 0, 2 * sizeof(uint32_t), stream), "qsdvr_ray_cut_noalloc: memset");
+    const uint32_t blocks = (pixel_count + kScanBlock - 1) / kScanBlock;
+    ray_cut_kernel<<<blocks, kScanBlock, 0, stream>>>(*camera, interval, pixel_count, mask, rays, origin, dir, sums);
+    scan_block_sums_kernel<<<1, 1024, 0, stream>>>(sums, blocks, totals);
+    ray_cut_apply_kernel<<<blocks, kScanBlock, 0, stream>>>(pixel_count, mask, rays, sums);
+    return check_launch("qsdvr_ray_cut_noalloc");
+}
