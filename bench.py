@@ -57,7 +57,7 @@ def dist_env():
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 20 ms during the timed region."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
 
@@ -79,7 +79,14 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, begin: bool):
+        """Record the wall-clock bounds of a timed region."""
+        if begin:
+            self.t0 = time.time()
+        else:
+            self.t1 = time.time()
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -90,22 +97,31 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
+        """Samples that arrived inside the timed window (plus one sampling period on each
+        side; the nearest two if the window is shorter than the sampling period)."""
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        parsed = []
+        for t, ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 7:
+            if len(parts) < 8:
                 continue
             try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
+                parsed.append((t, float(parts[1]), float(parts[2]), parts[4:8]))
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[3:7]):
+        t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", float("inf"))
+        inside = [q for q in parsed if t0 - 0.05 <= q[0] <= t1 + 0.05]
+        if len(inside) < 2 and parsed:
+            mid = 0.5 * (t0 + min(t1, parsed[-1][0]))
+            inside = sorted(parsed, key=lambda q: abs(q[0] - mid))[:2]
+        sm = [q[1] for q in inside]
+        reasons = set()
+        for q in inside:
+            for nm, v in zip(names, q[3]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": inside[0][2] if inside else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
 
 
 def measured_peak_hbm():
@@ -180,11 +196,13 @@ def samples_of(batch):
 
 # ----------------------------------------------------------------------------- timing
 
-def time_device(step, steps, warmup, stream):
+def time_device(step, steps, warmup, stream, clock=None):
     """Warm-up, then K steps between two events; also returns per-step kernel events."""
     for i in range(warmup):
         step(i, None)
     torch.cuda.synchronize()
+    if clock is not None:
+        clock.mark(True)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("timed")
@@ -194,6 +212,8 @@ def time_device(step, steps, warmup, stream):
     stop.record(stream)
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
+    if clock is not None:
+        clock.mark(False)
     total_ms = start.elapsed_time(stop)
     kern_ms = [a.elapsed_time(b) for a, b in ev]
     return total_ms, kern_ms
@@ -233,7 +253,8 @@ def run_ours(args, cfg, device, ws, rank):
     if ws > 1:
         torch.distributed.barrier()
     with ClockSampler(device.index) as clk:
-        total_ms, kern_ms = time_device(step, args.steps, args.warmup, stream)
+        time.sleep(0.3)  # nvidia-smi needs a moment before its first sample
+        total_ms, kern_ms = time_device(step, args.steps, args.warmup, stream, clk)
     if ws > 1:
         torch.distributed.barrier()
     # ---- e2e through the public API with host buffers (pinned), copies inside the region

@@ -220,7 +220,14 @@ typedef struct qsdvr_render_args {
     float *data_grad;         /* [(R+1)^3][32] accumulated */
     float *loss;              /* train: sum over rays of |color - target|^2 is added here */
     float grad_scale;         /* train: dL/dcolor = grad_scale * (color - target) */
+    void *workspace;          /* optional, 256-byte aligned: enables the persistent grid with     */
+    uint64_t workspace_bytes; /* dynamic ray scheduling and, in train, the per-warp row stash    */
 } qsdvr_render_args;
+
+/* Workspace bytes for qsdvr_render_* with these args on the current device (mode, storage
+ * and transmittance select the kernel; independent of ray_count).  One workspace must not
+ * be used by launches that may overlap on the GPU. */
+size_t qsdvr_render_workspace_size(const qsdvr_render_args *args);
 
 /* Replaces RenderGrid.forward (models/render.py:225-234, i.e. the SampleSDF, SampleNormal,
  * GridInterpolation, Shader and RayAggregate forwards) fused with GenerateRayPoints
@@ -233,6 +240,43 @@ int qsdvr_render_backward(const qsdvr_render_args *args, cudaStream_t stream);
 /* Forward + MSE loss gradient + backward in one launch (test.py:30-33 training step
  * without the optimizer): writes color, accumulates loss and gradients. */
 int qsdvr_render_train(const qsdvr_render_args *args, cudaStream_t stream);
+
+/* ---- fused grid optimizer ---------------------------------------------------------- */
+
+enum {
+    QSDVR_ADAM_ZERO_GRAD = 1,      /* write zeros over the gradient after using it           */
+    QSDVR_ADAM_SKIP_ZERO_GRAD = 2  /* leave elements whose gradient is exactly 0 untouched    */
+};
+
+/* One Adam step over `count` fp32 elements.  The default (flags without SKIP_ZERO_GRAD)
+ * is torch.optim.Adam's update, bias corrections included; `step` counts from 1.
+ * param_bf16, when not null, receives the updated parameters rounded to bf16 (the
+ * storage copy the fused render kernels read). */
+typedef struct qsdvr_adam_args {
+    float *param;
+    float *grad;
+    float *exp_avg;
+    float *exp_avg_sq;
+    void *param_bf16;   /* optional [count] bf16 */
+    uint64_t count;
+    double lr, beta1, beta2, eps; /* host precision; the kernel's float constants are derived from them */
+    uint32_t step;
+    int32_t flags;      /* QSDVR_ADAM_* */
+} qsdvr_adam_args;
+
+/* Replaces optimizer.step() + optimizer.zero_grad() of the reference's training loop
+ * (test.py:34-35, torch.optim.Adam over renderData and the layers) for grid parameters. */
+int qsdvr_adam_step(const qsdvr_adam_args *args, cudaStream_t stream);
+
+/* ---- FP64 loss for finite-difference gradient checks ---------------------------------- */
+
+/* sum_c (color_c - target_c)^2 per ray with every quantity in double (fixed mode: packed SH,
+ * vertex x + y(R+1) + z(R+1)^2); grids [R^3][8] and [(R+1)^3][32] in double.  The only FP64
+ * GPU code: central differences of it check qsdvr_render_backward / _train.  Restates the
+ * forward of RenderGrid (models/render.py:225-234) for one loss value per ray. */
+int qsdvr_render_loss_f64(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
+                          uint32_t reso, float interval, double logistic_coef, const double *sdf_grid,
+                          const double *data, const double *target, double *loss_per_ray, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

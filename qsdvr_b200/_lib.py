@@ -9,7 +9,7 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libqsdvr_b200.so")
+LIB_PATH = os.environ.get("QSDVR_B200_LIB") or os.path.join(_HERE, "libqsdvr_b200.so")
 
 P = ctypes.c_void_p
 U32 = ctypes.c_uint32

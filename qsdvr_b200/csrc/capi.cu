@@ -30,6 +30,8 @@ cudaError_t error_word_camera(unsigned *, int, cudaStream_t);
 cudaError_t error_word_surface(unsigned *, int, cudaStream_t);
 cudaError_t error_word_render(unsigned *, int, cudaStream_t);
 cudaError_t error_word_fused(unsigned *, int, cudaStream_t);
+cudaError_t error_word_optim(unsigned *, int, cudaStream_t);
+cudaError_t error_word_gradcheck(unsigned *, int, cudaStream_t);
 
 }  // namespace qsdvr
 
@@ -45,6 +47,8 @@ extern "C" int qsdvr_device_error(uint32_t *word, int clear, cudaStream_t stream
     if (e == cudaSuccess) e = error_word_surface(&w, clear, stream);
     if (e == cudaSuccess) e = error_word_render(&w, clear, stream);
     if (e == cudaSuccess) e = error_word_fused(&w, clear, stream);
+    if (e == cudaSuccess) e = error_word_optim(&w, clear, stream);
+    if (e == cudaSuccess) e = error_word_gradcheck(&w, clear, stream);
     *word = w;
     return check_cuda(e, "qsdvr_device_error");
 }

@@ -29,13 +29,53 @@ QSDVR_ERROR_WORD_ACCESSOR(fused)
 
 namespace {
 
-constexpr int kWarpsPerBlock = 4;
+// Tunables (compile-time).  One ray per warp; with one warp per block the block scheduler
+// balances ray lengths by itself.
+#ifndef QSDVR_FUSED_WARPS
+#define QSDVR_FUSED_WARPS 1
+#endif
+#ifndef QSDVR_FUSED_MIN_BLOCKS
+#define QSDVR_FUSED_MIN_BLOCKS 16
+#endif
+#ifndef QSDVR_GATHER_UNROLL
+#define QSDVR_GATHER_UNROLL 2
+#endif
+constexpr int kWarpsPerBlock = QSDVR_FUSED_WARPS;
+constexpr int kGatherUnroll = QSDVR_GATHER_UNROLL;
 constexpr int kThreads = kWarpsPerBlock * kWarp;
 constexpr int kRow = 36;          // floats per staged appearance row
 constexpr uint32_t kMaxChunks = 64;  // render samples per ray <= 2048
-constexpr int kC = 32;
 
 enum Pass { kForward = 0, kBackward = 1, kTrain = 2 };
+
+// Persistent train mode: each warp stashes the interpolated rows of the kSlotChunks chunks
+// before a ray's last one (the last stays in shared memory) so that the backward reloads
+// them from L2 instead of re-gathering 8 corner rows per sample from HBM.
+#ifndef QSDVR_SLOT_CHUNKS
+#define QSDVR_SLOT_CHUNKS 5
+#endif
+constexpr uint32_t kSlotChunks = QSDVR_SLOT_CHUNKS;
+constexpr uint32_t kChunkFloats = kWarp * 32;  // one chunk of rows in a slot (4 KiB, unpadded)
+
+// L2 evict_last for the stash: it is re-read shortly and must survive the streaming gathers.
+__device__ __forceinline__ uint64_t evict_last_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ void st4_keep(float *p, float4 v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(v.x), "f"(v.y),
+                 "f"(v.z), "f"(v.w), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ float4 ld4_keep(const float *p, uint64_t pol) {
+    float4 v;
+    asm volatile("ld.global.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(pol)
+                 : "memory");
+    return v;
+}
 
 struct Params {
     const qsdvr_ray_info *rays;
@@ -53,6 +93,8 @@ struct Params {
     float *data_grad;
     float *loss;
     float grad_scale;
+    uint32_t *ray_counter;  // persistent mode: next ray to take (zeroed before the launch)
+    float *slots;           // persistent train mode: per-warp row stash, kSlotChunks chunks each
 };
 
 // ---- storage access --------------------------------------------------------------------
@@ -122,7 +164,8 @@ struct Sample {
 // interpolated 32 channels in the warp's tile.
 template <bool kCompat, typename S>
 __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t nr, uint32_t chunk, int lane,
-                                           float *tile, Sample &s) {
+                                           float *tile, Sample &s, const float *from_slot = nullptr,
+                                           float *to_slot = nullptr) {
     const uint32_t R = p.R;
     const uint32_t i = chunk * kWarp + lane;
     const bool live = i < nr;
@@ -174,10 +217,27 @@ __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t
     const uint32_t R1 = R + 1;
     s.vbase = kCompat ? (uint32_t)s.cr.index
                       : (uint32_t)s.cr.cx + (uint32_t)s.cr.cy * R1 + (uint32_t)s.cr.cz * (R1 * R1);
+    const int q = lane & 7;
+    if (from_slot) {
+        // rows stashed by the forward: 32 rows x 128 B, 4 rows per warp instruction
+        const uint64_t pol = evict_last_policy();
+#pragma unroll
+        for (int st = 0; st < 8; ++st) {
+            const int j = st * 4 + (lane >> 3);
+            st4(tile + j * kRow + 4 * q, ld4_keep(from_slot + j * 32 + 4 * q, pol));
+        }
+        __syncwarp();
+        if (s.valid) {
+            s.rgb = shade<kCompat>(s.nrm, d, tile + lane * kRow, &s.spec);
+        } else {
+            s.rgb = f3{0.0f, 0.0f, 0.0f};
+            s.spec = f3{0.0f, 0.0f, 0.0f};
+        }
+        return;
+    }
     // gather: groups of 8 lanes fetch one sample's 8 corner rows, 4 samples per step
     const uint32_t sy = R1, sz = R1 * R1;
-    const int q = lane & 7;
-#pragma unroll 2
+#pragma unroll kGatherUnroll
     for (int st = 0; st < 8; ++st) {
         const int j = st * 4 + (lane >> 3);
         const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
@@ -196,17 +256,12 @@ __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t
             v = lerp4(a0, a1v, gz);
         }
         st4(tile + j * kRow + 4 * q, v);
+        if (to_slot) st4_keep(to_slot + j * 32 + 4 * q, v, evict_last_policy());
     }
     __syncwarp();
     if (s.valid) {
-        float dch[kC];
-        const float *row = tile + lane * kRow;
-#pragma unroll
-        for (int t = 0; t < 8; ++t) {
-            const float4 v = ld4(row + 4 * t);
-            dch[4 * t] = v.x; dch[4 * t + 1] = v.y; dch[4 * t + 2] = v.z; dch[4 * t + 3] = v.w;
-        }
-        s.rgb = shade<kCompat>(s.nrm, d, dch, &s.spec);
+        // the row stays in shared memory; the shader reads the channels it needs from it
+        s.rgb = shade<kCompat>(s.nrm, d, tile + lane * kRow, &s.spec);
     } else {
         s.rgb = f3{0.0f, 0.0f, 0.0f};
         s.spec = f3{0.0f, 0.0f, 0.0f};
@@ -332,14 +387,26 @@ __device__ __forceinline__ void red_cell(float *g8, uint32_t cell, const float *
 }
 
 template <bool kCompat, typename S, int kPass, bool kLogT>
-__global__ void __launch_bounds__(kThreads) render_kernel(const Params p) {
+__global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kernel(const Params p) {
     __shared__ __align__(16) float tiles[kWarpsPerBlock][kWarp * kRow];
-    __shared__ float block_sq[kWarpsPerBlock];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     float *tile = tiles[w];
-    const uint32_t r = blockIdx.x * kWarpsPerBlock + w;
+    const uint32_t warp_id = blockIdx.x * kWarpsPerBlock + w;
+    // Without a workspace each warp renders one ray (one warp per block: the block scheduler
+    // balances ray lengths).  With one, the grid is persistent and warps take rays from a
+    // counter; in train mode each warp also owns a row stash (slot).
+    const bool persistent = p.ray_counter != nullptr;
+    float *slot = (kPass == kTrain && p.slots) ? p.slots + (uint64_t)warp_id * kSlotChunks * kChunkFloats : nullptr;
     float sq = 0.0f;
-    if (r < p.n) {
+    uint32_t r = persistent ? 0u : warp_id;
+    for (;;) {
+    if (persistent) {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(p.ray_counter, 1u);
+        r = __shfl_sync(kFull, t, 0);
+    }
+    if (r >= p.n) break;
+    {
         const qsdvr_ray_info info = p.rays[r];
         const uint32_t ns = info.sdf_count;
         const uint32_t nr = ns > 1 ? ns - 1 : 0;
@@ -354,6 +421,7 @@ __global__ void __launch_bounds__(kThreads) render_kernel(const Params p) {
         Sample s;
         Transmittance<kLogT> tr;
         float ts_lo = 0.0f, ts_hi = 0.0f;  // transmittance carry at the start of chunk lane / lane+32
+        float T_last = 0.0f;               // transmittance of this lane's sample in the last chunk
         // ---------------- forward
         if (kPass != kBackward || run) {
             if (run) {
@@ -366,8 +434,12 @@ __global__ void __launch_bounds__(kThreads) render_kernel(const Params p) {
                         eval_alpha<S>(p, o, d, nr, c, lane, s);
                         tr.step(s.alpha, s.valid, lane);
                     } else {
-                        eval_chunk<kCompat, S>(p, o, d, nr, c, lane, tile, s);
+                        float *stash = (slot && c + 1 < chunks && c + 1 + kSlotChunks >= chunks)
+                                           ? slot + (c % kSlotChunks) * kChunkFloats
+                                           : nullptr;
+                        eval_chunk<kCompat, S>(p, o, d, nr, c, lane, tile, s, nullptr, stash);
                         const float T = tr.step(s.alpha, s.valid, lane);
+                        T_last = T;
                         acc.x += s.rgb.x * s.alpha * T;
                         acc.y += s.rgb.y * s.alpha * T;
                         acc.z += s.rgb.z * s.alpha * T;
@@ -383,7 +455,7 @@ __global__ void __launch_bounds__(kThreads) render_kernel(const Params p) {
         if (kPass == kTrain) {
             const f3 t = load3(p.target + 3ull * r);
             const f3 e{C.x - t.x, C.y - t.y, C.z - t.z};
-            if (lane == 0) sq = e.x * e.x + e.y * e.y + e.z * e.z;  // C is warp-uniform: count it once
+            if (lane == 0) sq += e.x * e.x + e.y * e.y + e.z * e.z;  // C is warp-uniform: count it once
             g = f3{p.grad_scale * e.x, p.grad_scale * e.y, p.grad_scale * e.z};
         } else if (kPass == kBackward) {
             g = load3(p.grad_color + 3ull * r);
@@ -393,10 +465,20 @@ __global__ void __launch_bounds__(kThreads) render_kernel(const Params p) {
             f3 suf{0.0f, 0.0f, 0.0f};  // compat: sum_{m>chunk} T a c ; fixed: R after the chunk
             float next_this = 0.0f;    // d_this term of the first sample of the following chunk
             for (int c = (int)chunks - 1; c >= 0; --c) {
-                const float t0 = __shfl_sync(kFull, c < 32 ? ts_lo : ts_hi, c & 31);
-                tr.carry = t0;
-                eval_chunk<kCompat, S>(p, o, d, nr, (uint32_t)c, lane, tile, s);
-                const float T = tr.step(s.alpha, s.valid, lane);
+                float T;
+                if (kPass == kTrain && c == (int)chunks - 1) {
+                    // the forward just evaluated this chunk: its rows are still in the tile and
+                    // its per-sample state in registers, so nothing is fetched again
+                    T = T_last;
+                } else {
+                    const float t0 = __shfl_sync(kFull, c < 32 ? ts_lo : ts_hi, c & 31);
+                    tr.carry = t0;
+                    const float *stashed = (slot && (uint32_t)c + 1 + kSlotChunks >= chunks)
+                                               ? slot + ((uint32_t)c % kSlotChunks) * kChunkFloats
+                                               : nullptr;
+                    eval_chunk<kCompat, S>(p, o, d, nr, (uint32_t)c, lane, tile, s, stashed);
+                    T = tr.step(s.alpha, s.valid, lane);
+                }
                 const float a = s.alpha;
                 const uint32_t i = (uint32_t)c * kWarp + lane;
                 float dl = 0.0f;  // dL/dalpha_i
@@ -468,17 +550,8 @@ __global__ void __launch_bounds__(kThreads) render_kernel(const Params p) {
                     quad_sdf_grad(a1, s.c1.u, (float)p.R, gs1, gq);
                     // rgb gradient -> shader backward (data gradient into the tile, normal gradient)
                     const f3 grgb{g.x * T * a, g.y * T * a, g.z * T * a};
-                    float dch[kC], gd[kC];
-                    float *row = tile + lane * kRow;
-#pragma unroll
-                    for (int t = 0; t < 8; ++t) {
-                        const float4 v = ld4(row + 4 * t);
-                        dch[4 * t] = v.x; dch[4 * t + 1] = v.y; dch[4 * t + 2] = v.z; dch[4 * t + 3] = v.w;
-                    }
-                    const f3 gn = shade_backward<kCompat>(grgb, s.nrm, d, dch, s.spec, gd);
-#pragma unroll
-                    for (int t = 0; t < 8; ++t)
-                        st4(row + 4 * t, make_float4(gd[4 * t], gd[4 * t + 1], gd[4 * t + 2], gd[4 * t + 3]));
+                    // data gradient written over the data row (every read precedes its write)
+                    const f3 gn = shade_backward_inplace<kCompat>(grgb, s.nrm, d, tile + lane * kRow, s.spec);
                     float ar[7], gr[6];
                     Store<S>::cell(p.sdf, (uint32_t)s.cr.index, ar);
                     quad_normal_grad(ar, s.cr.u, gn, gr);
@@ -505,16 +578,50 @@ __global__ void __launch_bounds__(kThreads) render_kernel(const Params p) {
             }
         }
     }
-    if (kPass == kTrain) {
-        sq = warp_sum(sq);
-        if (lane == 0) block_sq[w] = sq;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            float t = 0.0f;
-            for (int k = 0; k < kWarpsPerBlock; ++k) t += block_sq[k];
-            atomicAdd(p.loss, t);
-        }
+    if (!persistent) break;
+    }  // ray loop
+    if (kPass == kTrain && lane == 0 && sq != 0.0f) atomicAdd(p.loss, sq);
+}
+
+constexpr size_t kCounterBytes = 256;
+
+// Persistent grid and workspace size for the current device: one block per resident slot
+// of the train kernel (the heaviest instantiation, which bounds the others).
+struct Layout {
+    int error;
+    unsigned blocks;
+    size_t counter_bytes, train_bytes;
+};
+
+Layout layout_for(const qsdvr_render_args *a) {
+    Layout L{QSDVR_OK, 0, kCounterBytes, 0};
+    int dev = 0, sms = 0, per_sm = 0;
+    if (check_cuda(cudaGetDevice(&dev), "render: cudaGetDevice") != QSDVR_OK ||
+        check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "render: SM count") != QSDVR_OK) {
+        L.error = QSDVR_ERR_CUDA;
+        return L;
     }
+    const bool compat = a->mode == QSDVR_MODE_COMPAT;
+    const bool bf16 = a->storage == QSDVR_STORAGE_BF16;
+    const bool logt = a->transmittance == QSDVR_TRANSMITTANCE_LOG;
+    const void *fn;
+#define QSDVR_FN(C, S, L2) fn = reinterpret_cast<const void *>(&render_kernel<C, S, kTrain, L2>)
+    if (compat) {
+        if (bf16) { if (logt) QSDVR_FN(true, __nv_bfloat16, true); else QSDVR_FN(true, __nv_bfloat16, false); }
+        else { if (logt) QSDVR_FN(true, float, true); else QSDVR_FN(true, float, false); }
+    } else {
+        if (bf16) { if (logt) QSDVR_FN(false, __nv_bfloat16, true); else QSDVR_FN(false, __nv_bfloat16, false); }
+        else { if (logt) QSDVR_FN(false, float, true); else QSDVR_FN(false, float, false); }
+    }
+#undef QSDVR_FN
+    if (check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0), "render: occupancy") !=
+        QSDVR_OK) {
+        L.error = QSDVR_ERR_CUDA;
+        return L;
+    }
+    L.blocks = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
+    L.train_bytes = kCounterBytes + (size_t)L.blocks * kWarpsPerBlock * kSlotChunks * kChunkFloats * sizeof(float);
+    return L;
 }
 
 template <int kPass>
@@ -537,7 +644,21 @@ int launch(const qsdvr_render_args *a, cudaStream_t stream) {
     p.data_grad = a->data_grad;
     p.loss = a->loss;
     p.grad_scale = a->grad_scale;
-    const unsigned blocks = grid_for(a->ray_count, kWarpsPerBlock);
+    p.ray_counter = nullptr;
+    p.slots = nullptr;
+    unsigned blocks = grid_for(a->ray_count, kWarpsPerBlock);
+    if (a->workspace) {
+        const Layout L = layout_for(a);
+        if (L.error != QSDVR_OK) return L.error;
+        if (a->workspace_bytes < (kPass == kTrain ? L.train_bytes : L.counter_bytes))
+            return set_error(QSDVR_ERR_WORKSPACE, "render: workspace %llu < %zu bytes",
+                             (unsigned long long)a->workspace_bytes, kPass == kTrain ? L.train_bytes : L.counter_bytes);
+        p.ray_counter = static_cast<uint32_t *>(a->workspace);
+        if (kPass == kTrain) p.slots = reinterpret_cast<float *>(static_cast<char *>(a->workspace) + kCounterBytes);
+        const int st = check_cuda(cudaMemsetAsync(p.ray_counter, 0, sizeof(uint32_t), stream), "render: memset");
+        if (st != QSDVR_OK) return st;
+        blocks = L.blocks;
+    }
     const bool compat = a->mode == QSDVR_MODE_COMPAT;
     const bool bf16 = a->storage == QSDVR_STORAGE_BF16;
     const bool logt = a->transmittance == QSDVR_TRANSMITTANCE_LOG;
@@ -578,6 +699,8 @@ int validate(const qsdvr_render_args *a, int pass) {
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null grad_color");
     if (pass == kTrain && a->ray_count && (!a->target || !a->loss))
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null target or loss");
+    if (a->workspace && !aligned(a->workspace, 256))
+        return set_error(QSDVR_ERR_ALIGNMENT, "render: workspace needs 256-byte alignment");
     return QSDVR_OK;
 }
 
@@ -585,6 +708,12 @@ int validate(const qsdvr_render_args *a, int pass) {
 }  // namespace qsdvr
 
 using namespace qsdvr;
+
+extern "C" size_t qsdvr_render_workspace_size(const qsdvr_render_args *args) {
+    if (!args) return 0;
+    const Layout L = layout_for(args);
+    return L.error == QSDVR_OK ? L.train_bytes : 0;
+}
 
 extern "C" int qsdvr_render_forward(const qsdvr_render_args *args, cudaStream_t stream) {
     const int st = validate(args, kForward);

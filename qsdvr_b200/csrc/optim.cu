@@ -1,0 +1,110 @@
+// Fused grid optimizer: Adam on the FP32 master grids in one pass over HBM, optionally
+// refreshing the BF16 storage copy the render kernels read and zeroing the gradient for
+// the next step (the reference runs torch.optim.Adam then zero_grad, test.py:34-35).
+//
+// Per element: m = m + (1 - b1)(g - m); v = b2 v + (1 - b2) g^2;
+// p -= (lr / (1 - b1^t)) m / (sqrt(v) / sqrt(1 - b2^t) + eps)   (torch.optim.Adam's formula).
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace qsdvr {
+
+QSDVR_ERROR_WORD_ACCESSOR(optim)
+
+namespace {
+
+struct AdamParams {
+    float *param, *grad, *m, *v;
+    __nv_bfloat16 *copy;
+    uint64_t n;
+    float b1, b2, one_minus_b1, one_minus_b2, step_size, bc2_sqrt, eps;
+    bool zero_grad, skip_zero;
+};
+
+__device__ __forceinline__ void adam_one(float &p, float g, float &m, float &v, const AdamParams &a) {
+    m = m + a.one_minus_b1 * (g - m);       // lerp(m, g, 1 - b1)
+    v = __fmul_rn(v, a.b2);                  // v *= b2, then v += (1 - b2) g g
+    v = v + a.one_minus_b2 * g * g;
+    const float denom = sqrtf(v) / a.bc2_sqrt + a.eps;
+    p = p - a.step_size * (m / denom);
+}
+
+__global__ void __launch_bounds__(256) adam_kernel(const AdamParams a) {
+    const uint64_t n4 = a.n / 4;
+    const uint64_t stride = (uint64_t)gridDim.x * 256;
+    for (uint64_t i = blockIdx.x * 256ull + threadIdx.x; i < n4; i += stride) {
+        float4 g = ld4(a.grad + 4 * i);
+        if (a.skip_zero && g.x == 0.0f && g.y == 0.0f && g.z == 0.0f && g.w == 0.0f) continue;
+        float4 p = ld4(a.param + 4 * i), m = ld4(a.m + 4 * i), v = ld4(a.v + 4 * i);
+        if (!a.skip_zero || g.x != 0.0f) adam_one(p.x, g.x, m.x, v.x, a);
+        if (!a.skip_zero || g.y != 0.0f) adam_one(p.y, g.y, m.y, v.y, a);
+        if (!a.skip_zero || g.z != 0.0f) adam_one(p.z, g.z, m.z, v.z, a);
+        if (!a.skip_zero || g.w != 0.0f) adam_one(p.w, g.w, m.w, v.w, a);
+        st4(a.param + 4 * i, p);
+        st4(a.m + 4 * i, m);
+        st4(a.v + 4 * i, v);
+        if (a.zero_grad) st4(a.grad + 4 * i, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+        if (a.copy) {
+            __nv_bfloat162 lo = __floats2bfloat162_rn(p.x, p.y), hi = __floats2bfloat162_rn(p.z, p.w);
+            uint2 packed;
+            packed.x = *reinterpret_cast<uint32_t *>(&lo);
+            packed.y = *reinterpret_cast<uint32_t *>(&hi);
+            *reinterpret_cast<uint2 *>(a.copy + 4 * i) = packed;
+        }
+    }
+    // tail (n not a multiple of 4)
+    for (uint64_t i = 4 * n4 + blockIdx.x * 256ull + threadIdx.x; i < a.n; i += stride) {
+        const float g = a.grad[i];
+        if (a.skip_zero && g == 0.0f) continue;
+        float p = a.param[i], m = a.m[i], v = a.v[i];
+        adam_one(p, g, m, v, a);
+        a.param[i] = p;
+        a.m[i] = m;
+        a.v[i] = v;
+        if (a.zero_grad) a.grad[i] = 0.0f;
+        if (a.copy) a.copy[i] = __float2bfloat16_rn(p);
+    }
+}
+
+}  // namespace
+}  // namespace qsdvr
+
+using namespace qsdvr;
+
+extern "C" int qsdvr_adam_step(const qsdvr_adam_args *args, cudaStream_t stream) {
+    if (!args) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_adam_step: null args");
+    if (args->count == 0) return QSDVR_OK;
+    if (!args->param || !args->grad || !args->exp_avg || !args->exp_avg_sq)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_adam_step: null pointer");
+    if (!aligned(args->param, 16) || !aligned(args->grad, 16) || !aligned(args->exp_avg, 16) ||
+        !aligned(args->exp_avg_sq, 16) || (args->param_bf16 && !aligned(args->param_bf16, 8)))
+        return set_error(QSDVR_ERR_ALIGNMENT, "qsdvr_adam_step: buffers need 16-byte (copy 8-byte) alignment");
+    if (args->step == 0 || !(args->beta1 >= 0.0 && args->beta1 < 1.0) || !(args->beta2 >= 0.0 && args->beta2 < 1.0))
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_adam_step: step must be >= 1 and betas in [0,1)");
+    AdamParams a;
+    a.param = args->param;
+    a.grad = args->grad;
+    a.m = args->exp_avg;
+    a.v = args->exp_avg_sq;
+    a.copy = static_cast<__nv_bfloat16 *>(args->param_bf16);
+    a.n = args->count;
+    // constants rounded once from double, as torch.optim.Adam's scalars are
+    a.b1 = (float)args->beta1;
+    a.b2 = (float)args->beta2;
+    a.one_minus_b1 = (float)(1.0 - args->beta1);
+    a.one_minus_b2 = (float)(1.0 - args->beta2);
+    const double bc1 = 1.0 - pow(args->beta1, (double)args->step);
+    const double bc2 = 1.0 - pow(args->beta2, (double)args->step);
+    a.step_size = (float)(args->lr / bc1);
+    a.bc2_sqrt = (float)sqrt(bc2);
+    a.eps = (float)args->eps;
+    a.zero_grad = (args->flags & QSDVR_ADAM_ZERO_GRAD) != 0;
+    a.skip_zero = (args->flags & QSDVR_ADAM_SKIP_ZERO_GRAD) != 0;
+    const uint64_t work = (args->count + 3) / 4;
+    unsigned blocks = grid_for(work, 256);
+    const unsigned cap = 148u * 16;  // a few waves of resident blocks, grid-stride beyond
+    if (blocks > cap) blocks = cap;
+    adam_kernel<<<blocks, 256, 0, stream>>>(a);
+    return check_launch("qsdvr_adam_step");
+}

@@ -30,14 +30,28 @@ class RenderArgs(ctypes.Structure):
     _fields_ = [("rays", P), ("origin", P), ("dir", P), ("ray_count", U32), ("reso", U32), ("interval", F32),
                 ("logistic_coef", F32), ("mode", I32), ("storage", I32), ("transmittance", I32), ("reserved", I32),
                 ("sdf_grid", P), ("data", P), ("color", P), ("target", P), ("grad_color", P), ("sdf_grad", P),
-                ("data_grad", P), ("loss", P), ("grad_scale", F32)]
+                ("data_grad", P), ("loss", P), ("grad_scale", F32), ("workspace", P), ("workspace_bytes", ctypes.c_uint64)]
 
 
 _lib.extra_signatures({
     "qsdvr_render_forward": [ctypes.POINTER(RenderArgs), P],
     "qsdvr_render_backward": [ctypes.POINTER(RenderArgs), P],
     "qsdvr_render_train": [ctypes.POINTER(RenderArgs), P],
-})
+}, {"qsdvr_render_workspace_size": [ctypes.POINTER(RenderArgs)]})
+
+_workspaces: dict = {}
+
+
+def workspace(device, args: "RenderArgs") -> torch.Tensor:
+    """A cached workspace for the persistent kernels on ``device`` (one per device and
+    kernel configuration; launches on one stream never overlap, so it can be reused)."""
+    key = (device, args.mode, args.storage, args.transmittance)
+    need = int(_lib.lib().qsdvr_render_workspace_size(ctypes.byref(args)))
+    ws = _workspaces.get(key)
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(need, dtype=torch.uint8, device=device)
+        _workspaces[key] = ws
+    return ws
 
 
 def _ptr(t):
@@ -69,7 +83,7 @@ def _grid_storage(sdf_grid, data, R):
 
 def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat", transmittance="product",
               color=None, target=None, grad_color=None, sdf_grad=None, data_grad=None, loss=None,
-              grad_scale=0.0) -> RenderArgs:
+              grad_scale=0.0, persistent=True) -> RenderArgs:
     dev, n = _check_batch(rays, origin, direction)
     a = RenderArgs()
     a.rays, a.origin, a.dir = _ptr(rays), _ptr(origin), _ptr(direction)
@@ -82,6 +96,11 @@ def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="
     a.color, a.target, a.grad_color = _ptr(color), _ptr(target), _ptr(grad_color)
     a.sdf_grad, a.data_grad, a.loss = _ptr(sdf_grad), _ptr(data_grad), _ptr(loss)
     a.grad_scale = float(grad_scale)
+    a.workspace, a.workspace_bytes = None, 0
+    if persistent and n:
+        with torch.cuda.device(dev):
+            ws = workspace(dev, a)
+        a.workspace, a.workspace_bytes = ws.data_ptr(), ws.numel()
     return a
 
 
@@ -90,19 +109,20 @@ def _stream(dev):
 
 
 def render_forward(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat",
-                   transmittance="product", color=None):
+                   transmittance="product", color=None, persistent=True):
     """Colour of every ray [N,3]."""
     dev, n = _check_batch(rays, origin, direction)
     if color is None:
         color = torch.empty((n, 3), dtype=torch.float32, device=dev)
-    a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color)
+    a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color,
+                  persistent=persistent)
     with torch.cuda.device(dev):
         call("qsdvr_render_forward", ctypes.byref(a), _stream(dev))
     return color
 
 
 def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
-                    mode="compat", transmittance="product"):
+                    mode="compat", transmittance="product", persistent=True):
     """Accumulate dL/d(sdf_grid) and dL/d(data) (fp32) for a given dL/dcolor."""
     dev, n = _check_batch(rays, origin, direction)
     for t, nm, shape in ((sdf_grad, "sdf_grad", sdf_grid.numel()), (data_grad, "data_grad", data.numel())):
@@ -110,13 +130,13 @@ def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, i
             raise ValueError(f"{nm} must be a contiguous float32 tensor shaped like its grid")
     g = grad_color.contiguous().float()
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, grad_color=g,
-                  sdf_grad=sdf_grad, data_grad=data_grad)
+                  sdf_grad=sdf_grad, data_grad=data_grad, persistent=persistent)
     with torch.cuda.device(dev):
         call("qsdvr_render_backward", ctypes.byref(a), _stream(dev))
 
 
 def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
-                 mode="compat", transmittance="product", loss=None, color=None):
+                 mode="compat", transmittance="product", loss=None, color=None, persistent=True):
     """Forward + MSE (mean over N x 3) + backward in one launch.  Returns (color, loss_sum)
     where loss_sum accumulates sum |color - target|^2 (divide by 3N for the mean)."""
     dev, n = _check_batch(rays, origin, direction)
@@ -126,7 +146,7 @@ def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval
         loss = torch.zeros(1, dtype=torch.float32, device=dev)
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color,
                   target=target.contiguous(), sdf_grad=sdf_grad, data_grad=data_grad, loss=loss,
-                  grad_scale=2.0 / (3.0 * max(n, 1)))
+                  grad_scale=2.0 / (3.0 * max(n, 1)), persistent=persistent)
     with torch.cuda.device(dev):
         call("qsdvr_render_train", ctypes.byref(a), _stream(dev))
     return color, loss

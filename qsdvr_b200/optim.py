@@ -1,0 +1,72 @@
+"""Fused grid optimizer (qsdvr_adam_step): torch.optim.Adam's update for grid parameters
+in one HBM pass, with the gradient zeroed and the bf16 storage copy refreshed in the same
+pass.  Replaces ``optimizer.step(); optimizer.zero_grad()`` of the reference's training
+loop (test.py:34-35) for the grids."""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import I32, P, U32, U64, call
+
+ZERO_GRAD = 1
+SKIP_ZERO_GRAD = 2
+
+
+class AdamArgs(ctypes.Structure):
+    """qsdvr_adam_args (include/qsdvr_b200.h)."""
+    _fields_ = [("param", P), ("grad", P), ("exp_avg", P), ("exp_avg_sq", P), ("param_bf16", P), ("count", U64),
+                ("lr", ctypes.c_double), ("beta1", ctypes.c_double), ("beta2", ctypes.c_double),
+                ("eps", ctypes.c_double), ("step", U32), ("flags", I32)]
+
+
+_lib.extra_signatures({"qsdvr_adam_step": [ctypes.POINTER(AdamArgs), P]})
+
+
+def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, betas=(0.9, 0.999), eps=1e-8, param_bf16=None,
+              zero_grad=True, skip_zero_grad=False):
+    for t, nm in ((param, "param"), (grad, "grad"), (exp_avg, "exp_avg"), (exp_avg_sq, "exp_avg_sq")):
+        if not t.is_cuda or t.dtype != torch.float32 or not t.is_contiguous() or t.numel() != param.numel():
+            raise ValueError(f"{nm} must be a contiguous CUDA float32 tensor shaped like param")
+    if param_bf16 is not None and (param_bf16.dtype != torch.bfloat16 or param_bf16.numel() != param.numel()):
+        raise ValueError("param_bf16 must be a bfloat16 tensor shaped like param")
+    a = AdamArgs()
+    a.param, a.grad, a.exp_avg, a.exp_avg_sq = param.data_ptr(), grad.data_ptr(), exp_avg.data_ptr(), exp_avg_sq.data_ptr()
+    a.param_bf16 = param_bf16.data_ptr() if param_bf16 is not None else None
+    a.count = param.numel()
+    a.lr, a.beta1, a.beta2, a.eps = float(lr), float(betas[0]), float(betas[1]), float(eps)
+    a.step = int(step)
+    a.flags = (ZERO_GRAD if zero_grad else 0) | (SKIP_ZERO_GRAD if skip_zero_grad else 0)
+    with torch.cuda.device(param.device):
+        call("qsdvr_adam_step", ctypes.byref(a), ctypes.c_void_p(torch.cuda.current_stream(param.device).cuda_stream))
+
+
+class FusedGridAdam(torch.optim.Optimizer):
+    """Adam for grid parameters using the fused kernel.  ``step()`` also zeroes the
+    gradients (so ``zero_grad()`` is a no-op) and, for parameters registered with a bf16
+    copy via ``bf16_copies={param: copy}``, refreshes the copy."""
+
+    def __init__(self, params, lr=1e-2, betas=(0.9, 0.999), eps=1e-8, bf16_copies=None, skip_zero_grad=False):
+        super().__init__(params, dict(lr=lr, betas=betas, eps=eps))
+        self.bf16_copies = bf16_copies or {}
+        self.skip_zero_grad = skip_zero_grad
+
+    def zero_grad(self, set_to_none: bool = False):
+        pass  # step() already wrote zeros over the gradients it consumed
+
+    @torch.no_grad()
+    def step(self, closure=None):
+        for group in self.param_groups:
+            for p in group["params"]:
+                if p.grad is None:
+                    continue
+                st = self.state[p]
+                if not st:
+                    st["step"] = 0
+                    st["exp_avg"] = torch.zeros_like(p, memory_format=torch.contiguous_format)
+                    st["exp_avg_sq"] = torch.zeros_like(p, memory_format=torch.contiguous_format)
+                st["step"] += 1
+                adam_step(p.data, p.grad, st["exp_avg"], st["exp_avg_sq"], st["step"], group["lr"], group["betas"],
+                          group["eps"], self.bf16_copies.get(p), True, self.skip_zero_grad)

@@ -192,3 +192,26 @@ def test_rays_outside_grid_are_flagged_not_faulting(fz):
     assert torch.isfinite(img).all()
     assert img[2].abs().max().item() == 0.0
     assert _lib.device_error() & _lib.DEVERR_INDEX
+
+
+@pytest.mark.parametrize("mode", ["compat", "fixed"])
+def test_persistent_stash_path_matches_one_ray_per_block(fz, mode):
+    """The persistent grid (dynamic ray scheduling, per-warp row stash reloaded in the
+    backward) gives the same colours, loss and gradients as one ray per block."""
+    from qsdvr_b200 import scenes
+
+    R, k, interval = 40, 12.0, 4.0 / 320  # rays up to ~250 samples: 8 chunks, beyond the stash
+    cam = camera_batch((2.0, 3.1, -1.7), 72, 100.0, interval, R)
+    grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.55, 0.01, seed=9).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=9).to(DEV)
+    target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(9)).to(DEV)
+    out = []
+    for persistent in (False, True):
+        sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+        col, loss = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k, sg,
+                                    dg, mode=mode, persistent=persistent)
+        out.append((col, loss, sg, dg))
+    (c0, l0, s0, d0), (c1, l1, s1, d1) = out
+    assert (c0 - c1).abs().max().item() < 1e-6
+    assert abs(l0.item() - l1.item()) < 1e-5 * max(1.0, l0.item())
+    assert rel_err(s1.cpu(), s0.cpu()) < 1e-5 and rel_err(d1.cpu(), d0.cpu()) < 1e-5
