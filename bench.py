@@ -40,8 +40,22 @@ WORKLOADS = {
                      storage="bf16"),
     "plain128": dict(R=128, rays=8192, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
                      storage="f32"),
+    # SH degree 3 (64-channel rows, fixed mode): the configs' appearance model
+    "sh3_256": dict(R=256, rays=65536, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
+                    storage="f32", sh=3),
+    "sh3_bf16_256": dict(R=256, rays=65536, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
+                         storage="bf16", sh=3),
+    "sh3_128": dict(R=128, rays=8192, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
+                    storage="f32", sh=3),
 }
-BYTES_PER_SAMPLE = {"f32": 3264, "bf16": 2240}  # algorithmic bytes per render sample (3-pass model)
+
+
+def bytes_per_sample(storage: str, sh: int) -> int:
+    """Algorithmic bytes per render sample (3-pass model): forward gather 8 C b, backward
+    re-gather 8 C b, gradient scatter 8 C 4, quadric cells 192 (C channels, b storage bytes)."""
+    c = 32 if sh == 2 else 64
+    b = 4 if storage == "f32" else 2
+    return 8 * c * b * 2 + 8 * c * 4 + 192
 BYTES_PER_RAY = 64  # origin + dir in, target in, colour out, RayInfo
 K_LOGISTIC = 5.0
 METRIC = "train rays/s fwd+bwd @256^3 grid (256 samples/ray, 65536-ray batches)"
@@ -155,9 +169,10 @@ def build_scene(cfg, device, seed):
 
     R = cfg["R"]
     gt_sdf = fused.pad_grid7(scenes.procedural_grid(R, seed=seed, device=device).reshape(-1, 7))
-    gt_data = scenes.appearance(R, seed=seed, device=device, procedural=True)
+    sh = cfg.get("sh", 2)
+    gt_data = scenes.appearance(R, seed=seed, device=device, procedural=True, sh_degree=sh)
     sdf = fused.pad_grid7(scenes.sphere_grid(R, 0.5, 0.01, seed=seed, device=device).reshape(-1, 7))
-    data = scenes.appearance(R, seed=seed + 1, device=device)
+    data = scenes.appearance(R, seed=seed + 1, device=device, sh_degree=sh)
     cams = scenes.hemisphere_cameras(cfg["views"], cfg["radius"], cfg["size"], cfg["size"], cfg["focal"], 2.0, 6.0,
                                      seed=seed)
     rays, origin, direction = [], [], []
@@ -228,6 +243,7 @@ def run_ours(args, cfg, device, ws, rank):
     batches = make_batches(scene, cfg, 8, device, seed=1000 + rank)
     sdf, data = scene["model"]
     transmittance = "log" if storage == "bf16" else "product"
+    mode = "compat" if cfg.get("sh", 2) == 2 else "fixed"
     if storage == "bf16":
         sdf_k, data_k = sdf.to(torch.bfloat16), data.to(torch.bfloat16)
     else:
@@ -246,7 +262,7 @@ def run_ours(args, cfg, device, ws, rank):
         if ev is not None:
             ev[0].record(stream)
         fused.render_train(b["target"], b["rays"], b["origin"], b["dir"], sdf_k, data_k, R, cfg["interval"],
-                           K_LOGISTIC, sg, dg, "compat", transmittance, loss=loss, color=color)
+                           K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color)
         if ev is not None:
             ev[1].record(stream)
 
@@ -275,7 +291,7 @@ def run_ours(args, cfg, device, ws, rank):
         if ev is not None:
             ev[0].record(stream)
         fused.render_train(dev_in["target"], dev_in["rays"], dev_in["origin"], dev_in["dir"], sdf_k, data_k, R,
-                           cfg["interval"], K_LOGISTIC, sg, dg, "compat", transmittance, loss=loss, color=color)
+                           cfg["interval"], K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color)
         if ev is not None:
             ev[1].record(stream)
         loss_host.copy_(loss, non_blocking=True)
@@ -296,7 +312,8 @@ def run_ours(args, cfg, device, ws, rank):
     # ---- roofline of the train kernel
     samples = [samples_of(b) for b in batches]
     mean_samples = sum(samples) / len(samples)
-    alg_bytes = mean_samples * BYTES_PER_SAMPLE[storage] + cfg["rays"] * BYTES_PER_RAY
+    bps = bytes_per_sample(storage, cfg.get("sh", 2))
+    alg_bytes = mean_samples * bps + cfg["rays"] * BYTES_PER_RAY
     achieved = alg_bytes / (kern_avg / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
     tps = profiled_traffic_per_sample(storage)
@@ -308,7 +325,8 @@ def run_ours(args, cfg, device, ws, rank):
         "data": "synthetic (seeded procedural scene, random-init sphere model)",
         "config": {"workload": f"{args.workload}: R={R}^3 quadric + ({R + 1})^3x32 appearance grid, {storage}, "
                                f"{cfg['rays']} random rays/step from {cfg['views']} views at {cfg['size']}^2, "
-                               f"interval {cfg['interval']:.6g} (256 samples/ray), compat mode, k={K_LOGISTIC}",
+                               f"interval {cfg['interval']:.6g} (256 samples/ray), SH degree {cfg.get('sh', 2)}, "
+                               f"{mode} mode, k={K_LOGISTIC}",
                    "global_batch": cfg["rays"] * ws, "samples_per_step": round(mean_samples),
                    "step": "zero grads + fused forward/MSE/backward launch",
                    "l2": "inputs larger than L2 (grids 2.7 GB), no flush", "parallelism": f"replicas x{ws}"},
@@ -318,11 +336,11 @@ def run_ours(args, cfg, device, ws, rank):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None if traffic is None else round(traffic),
                      "kernel": "render_kernel<train>", "kernel_ms": round(kern_avg, 4),
-                     "algorithmic_bytes": round(alg_bytes), "bytes_per_sample": BYTES_PER_SAMPLE[storage],
+                     "algorithmic_bytes": round(alg_bytes), "bytes_per_sample": bps,
                      "peak_kind": peak_kind},
         "clocks": clk.summary(),
     }
-    if ws == 1 and not args.no_cpu_baseline:
+    if ws == 1 and not args.no_cpu_baseline and cfg.get("sh", 2) == 2:  # the reference's CPU path is SH degree 2
         out["cpu_baseline"] = cpu_baseline(scene, batches[0], cfg, args.cpu_rays)
     return out
 
@@ -379,6 +397,9 @@ def cpu_baseline(scene, batch, cfg, n_rays, steps=1):
 
 def run_reference(args, cfg):
     """The reference's CPU implementation timed on the host cores (rank 0 only)."""
+    if cfg.get("sh", 2) != 2:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference renders SH degree 2 only"}))
+        return
     torch.set_num_threads(os.cpu_count() or 1)
     device = torch.device("cuda", 0) if torch.cuda.is_available() else None
     if device is None:

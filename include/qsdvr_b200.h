@@ -197,7 +197,8 @@ enum {
  * unit direction); samples are generated on the fly exactly as GenerateRayPoints
  * (kernel/camera.cu:60-96) would.  Only sdf_count of each record is read.
  *   sdf_grid: [R^3][8] (a0..a6 + one pad) in `storage` precision, cell x + yR + zR^2;
- *   data:     [(R+1)^3][32] appearance rows in `storage` precision;
+ *   data:     [(R+1)^3][C] appearance rows in `storage` precision, C = 32 (SH degree 2)
+ *             or 64 (degree 3);
  *   grads:    fp32, same layouts, accumulated with atomics (caller zeroes). */
 typedef struct qsdvr_render_args {
     const qsdvr_ray_info *rays;
@@ -210,14 +211,15 @@ typedef struct qsdvr_render_args {
     int32_t mode;             /* QSDVR_MODE_* */
     int32_t storage;          /* QSDVR_STORAGE_* of sdf_grid and data */
     int32_t transmittance;    /* QSDVR_TRANSMITTANCE_* */
-    int32_t reserved;
+    int32_t sh_degree;        /* 2 (0 means 2; 32-channel rows, the reference) or 3 (fixed mode only,
+                                 64-channel rows: 16x3 SH, diffuse 48..50, metallic 51, ao 52) */
     const void *sdf_grid;
     const void *data;
     float *color;             /* [ray_count][3] output of forward / train */
     const float *target;      /* [ray_count][3] train: MSE target */
     const float *grad_color;  /* [ray_count][3] backward: dL/dcolor */
     float *sdf_grad;          /* [R^3][8] accumulated */
-    float *data_grad;         /* [(R+1)^3][32] accumulated */
+    float *data_grad;         /* [(R+1)^3][C] accumulated */
     float *loss;              /* train: sum over rays of |color - target|^2 is added here */
     float grad_scale;         /* train: dL/dcolor = grad_scale * (color - target) */
     void *workspace;          /* optional, 256-byte aligned: enables the persistent grid with     */

@@ -253,6 +253,34 @@ def sh_basis(v: torch.Tensor):
                         f[6] * (2.0 * y * y - z * z - x * x), f[7] * y * z, f[8] * (z * z - x * x)], 1)
 
 
+# Degree-3 extension (not in the reference): the reference's degree-2 basis treats y as the
+# polar axis with (z, x) spanning the azimuthal plane; band 3 follows the same convention with
+# the real-SH normalisations sqrt(35/(32 pi)), sqrt(105/(4 pi)), sqrt(21/(32 pi)),
+# sqrt(7/(16 pi)), sqrt(105/(16 pi)).
+SH3_A, SH3_B, SH3_C, SH3_D, SH3_E = (0.59004358992664351034, 2.89061144264055405538, 0.45704579946446573616,
+                                     0.37317633259011539141, 1.44530572132027702769)
+
+
+def sh_basis3(v: torch.Tensor):
+    """16 basis values at v: the 9 of sh_basis plus band 3."""
+    x, y, z = v[:, 0], v[:, 1], v[:, 2]
+    b3 = torch.stack([SH3_A * x * (3 * z * z - x * x), SH3_B * x * y * z, SH3_C * x * (4 * y * y - z * z - x * x),
+                      SH3_D * y * (2 * y * y - 3 * z * z - 3 * x * x), SH3_C * z * (4 * y * y - z * z - x * x),
+                      SH3_E * y * (z * z - x * x), SH3_A * z * (z * z - 3 * x * x)], 1)
+    return torch.cat([sh_basis(v), b3], 1)
+
+
+def shader_sh3(normal, view, data):
+    """Degree-3 shading: SH 16x3 packed at 0..47, diffuse 48..50, metallic 51, ao 52."""
+    normal = _t(normal)
+    view = _t(view).to(normal.dtype)
+    vdotn = (view * normal).sum(1, keepdim=True)
+    reflect = view - normal * (2.0 * vdotn)
+    spec = (sh_basis3(reflect).unsqueeze(-1) * data[:, :48].reshape(-1, 16, 3)).sum(1)
+    diffuse, metallic, ao = data[:, 48:51], data[:, 51:52], data[:, 52:53]
+    return (diffuse * (1.0 - metallic) + spec * metallic) * ao
+
+
 def sh_coefficients(data: torch.Tensor, compat: bool):
     """[M,9,3] SH coefficients: overlapping reads (render.cu:166-169) or packed."""
     if compat:
@@ -415,7 +443,7 @@ def vertex_index(cell_index: torch.Tensor, R: int, compat: bool):
     return x + y * (R + 1) + z * (R + 1) * (R + 1)
 
 
-def render(sdf_grid7, data, inputs: dict, k: float, compat: bool = True):
+def render(sdf_grid7, data, inputs: dict, k: float, compat: bool = True, sh_degree: int = 2):
     """The reference RenderGrid.forward (models/render.py:225-234) on a dense quadric grid.
 
     sdf_grid7: [R,R,R,7] (or [R^3,7]); data: [(R+1)^3, 32]; inputs: the dict of sample
@@ -427,6 +455,9 @@ def render(sdf_grid7, data, inputs: dict, k: float, compat: bool = True):
     normal = sample_normal(g7, inputs["renderPointList"], inputs["renderIndexList"])
     vidx = vertex_index(inputs["renderIndexList"], R, compat)
     d = grid_interpolation(data.reshape(-1, data.shape[-1]), inputs["renderPointList"], vidx, R + 1)
-    rgb = shade(normal, _t(inputs["viewDirList"]).to(DTYPE), d, compat)
+    if sh_degree == 3:
+        rgb = shader_sh3(normal, _t(inputs["viewDirList"]).to(DTYPE), d)
+    else:
+        rgb = shade(normal, _t(inputs["viewDirList"]).to(DTYPE), d, compat)
     color, _, _ = ray_aggregate(rgb, sdf, inputs["rayList"], k)
     return color

@@ -43,7 +43,16 @@ namespace {
 constexpr int kWarpsPerBlock = QSDVR_FUSED_WARPS;
 constexpr int kGatherUnroll = QSDVR_GATHER_UNROLL;
 constexpr int kThreads = kWarpsPerBlock * kWarp;
-constexpr int kRow = 36;          // floats per staged appearance row
+// Per SH degree: channels per row (32 or 64), staged row stride (+4 floats keeps both the
+// row-wise and the lane-wise float4 accesses bank-conflict free), lanes per sample in the
+// gather/scatter (one float4 each) and samples per warp instruction.
+template <int kDeg>
+struct Rows {
+    static constexpr int kC = ShLayout<kDeg>::kChannels;
+    static constexpr int kStride = kC + 4;
+    static constexpr int kLanes = kC / 4;
+    static constexpr int kPerStep = kWarp / kLanes;
+};
 constexpr uint32_t kMaxChunks = 64;  // render samples per ray <= 2048
 
 enum Pass { kForward = 0, kBackward = 1, kTrain = 2 };
@@ -55,7 +64,8 @@ enum Pass { kForward = 0, kBackward = 1, kTrain = 2 };
 #define QSDVR_SLOT_CHUNKS 5
 #endif
 constexpr uint32_t kSlotChunks = QSDVR_SLOT_CHUNKS;
-constexpr uint32_t kChunkFloats = kWarp * 32;  // one chunk of rows in a slot (4 KiB, unpadded)
+template <int kDeg>
+__host__ __device__ constexpr uint32_t chunk_floats() { return kWarp * Rows<kDeg>::kC; }  // rows of one chunk
 
 // L2 evict_last for the stash: it is re-read shortly and must survive the streaming gathers.
 __device__ __forceinline__ uint64_t evict_last_policy() {
@@ -113,8 +123,8 @@ struct Store<float> {
         a[0] = lo.x; a[1] = lo.y; a[2] = lo.z; a[3] = lo.w;
         a[4] = hi.x; a[5] = hi.y; a[6] = hi.z;
     }
-    __device__ static float4 quad(const void *d, uint32_t v, int q) {
-        return ld4(static_cast<const float *>(d) + 32ull * v + 4 * q);
+    __device__ static float4 quad(const void *d, uint32_t v, int q, int C) {
+        return ld4(static_cast<const float *>(d) + (uint64_t)C * v + 4 * q);
     }
 };
 
@@ -125,8 +135,9 @@ struct Store<__nv_bfloat16> {
         a[0] = bf_lo(r.x); a[1] = bf_hi(r.x); a[2] = bf_lo(r.y); a[3] = bf_hi(r.y);
         a[4] = bf_lo(r.z); a[5] = bf_hi(r.z); a[6] = bf_lo(r.w);
     }
-    __device__ static float4 quad(const void *d, uint32_t v, int q) {
-        const uint2 r = *reinterpret_cast<const uint2 *>(static_cast<const __nv_bfloat16 *>(d) + 32ull * v + 4 * q);
+    __device__ static float4 quad(const void *d, uint32_t v, int q, int C) {
+        const uint2 r =
+            *reinterpret_cast<const uint2 *>(static_cast<const __nv_bfloat16 *>(d) + (uint64_t)C * v + 4 * q);
         return make_float4(bf_lo(r.x), bf_hi(r.x), bf_lo(r.y), bf_hi(r.y));
     }
 };
@@ -147,6 +158,30 @@ __device__ __forceinline__ bool cell_in_grid(const CellPoint &c, uint32_t R) {
     return (unsigned)c.cx < R && (unsigned)c.cy < R && (unsigned)c.cz < R;
 }
 
+// alpha of one interval (kernel/render.cu:244).  compat: the reference's expression.
+// fixed: the same value, with the limits taken where exp(-k sdf) overflows (alpha -> 1 when
+// only the far end overflows, 0 when both do) instead of inf/inf.
+template <bool kCompat>
+__device__ __forceinline__ float interval_alpha(float e0, float e1) {
+    if (!kCompat && isinf(e1)) return isinf(e0) ? 0.0f : 1.0f;
+    return fmaxf((e1 - e0) / (1.0f + e1), 0.0f);
+}
+
+// d alpha / d sdf_{i+1} and d alpha / d sdf_i (kernel/render.cu:271-273).  fixed mode uses
+// q = 1 / (1 + e1), e1 q = 1 - q, which stays finite (and tends to 0) when e1 overflows.
+template <bool kCompat>
+__device__ __forceinline__ void interval_dalpha(float e0, float e1, float k, float *d_next, float *d_this) {
+    if (kCompat) {
+        const float inv = 1.0f / (1.0f + e1);
+        *d_next = -k * e1 * (1.0f + e0) * inv * inv;
+        *d_this = k * e0 * inv;
+    } else {
+        const float q = 1.0f / (1.0f + e1);
+        *d_next = -k * (1.0f + e0) * q * (1.0f - q);
+        *d_this = k * e0 * q;
+    }
+}
+
 // Per-lane state of one render sample of a chunk.
 struct Sample {
     bool valid;      // sample exists and all its cells are inside the grid
@@ -162,10 +197,12 @@ struct Sample {
 // Forward evaluation of render sample i = chunk*32 + lane (kernel/camera.cu:60-96,
 // kernel/surface.cu:54-115, kernel/render.cu:98-179, :239-244).  Leaves the sample's
 // interpolated 32 channels in the warp's tile.
-template <bool kCompat, typename S>
+template <bool kCompat, typename S, int kDeg>
 __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t nr, uint32_t chunk, int lane,
                                            float *tile, Sample &s, const float *from_slot = nullptr,
                                            float *to_slot = nullptr) {
+    using RW = Rows<kDeg>;
+    constexpr int kC = RW::kC, kRow = RW::kStride, kL = RW::kLanes, kPS = RW::kPerStep;
     const uint32_t R = p.R;
     const uint32_t i = chunk * kWarp + lane;
     const bool live = i < nr;
@@ -206,10 +243,13 @@ __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t
         s.nrm = f3{0.0f, 0.0f, 1.0f};
     }
     if (live && !ok) flag_error(QSDVR_DEVERR_INDEX);
+    // fixed mode: a sample whose first-order distance is not finite (|grad f| = 0 in a cell)
+    // is empty; compat keeps the reference's arithmetic, non-finite values included
+    if (!kCompat && !(isfinite(s0) && isfinite(s1))) ok = false;
     s.valid = ok;
     s.e0 = expf(-p.k * s0);
     s.e1 = expf(-p.k * s1);
-    s.alpha = ok ? fmaxf((s.e1 - s.e0) / (1.0f + s.e1), 0.0f) : 0.0f;
+    s.alpha = ok ? interval_alpha<kCompat>(s.e0, s.e1) : 0.0f;
     // trilinear weights and base vertex (kernel/render.cu:107-111)
     s.wx = (s.cr.u.x + 1.0f) / 2.0f;
     s.wy = (s.cr.u.y + 1.0f) / 2.0f;
@@ -217,51 +257,53 @@ __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t
     const uint32_t R1 = R + 1;
     s.vbase = kCompat ? (uint32_t)s.cr.index
                       : (uint32_t)s.cr.cx + (uint32_t)s.cr.cy * R1 + (uint32_t)s.cr.cz * (R1 * R1);
-    const int q = lane & 7;
+    const int q = lane % kL;
     if (from_slot) {
-        // rows stashed by the forward: 32 rows x 128 B, 4 rows per warp instruction
+        // rows stashed by the forward, one row per kL lanes per warp instruction
         const uint64_t pol = evict_last_policy();
 #pragma unroll
-        for (int st = 0; st < 8; ++st) {
-            const int j = st * 4 + (lane >> 3);
-            st4(tile + j * kRow + 4 * q, ld4_keep(from_slot + j * 32 + 4 * q, pol));
+        for (int st = 0; st < kL; ++st) {
+            const int j = st * kPS + lane / kL;
+            st4(tile + j * kRow + 4 * q, ld4_keep(from_slot + j * kC + 4 * q, pol));
         }
         __syncwarp();
         if (s.valid) {
-            s.rgb = shade<kCompat>(s.nrm, d, tile + lane * kRow, &s.spec);
+            s.rgb = shade_any<kCompat, kDeg>(s.nrm, d, tile + lane * kRow, &s.spec);
         } else {
             s.rgb = f3{0.0f, 0.0f, 0.0f};
             s.spec = f3{0.0f, 0.0f, 0.0f};
         }
         return;
     }
-    // gather: groups of 8 lanes fetch one sample's 8 corner rows, 4 samples per step
+    // gather: groups of kL lanes fetch one sample's 8 corner rows, kPS samples per step
     const uint32_t sy = R1, sz = R1 * R1;
 #pragma unroll kGatherUnroll
-    for (int st = 0; st < 8; ++st) {
-        const int j = st * 4 + (lane >> 3);
+    for (int st = 0; st < kL; ++st) {
+        const int j = st * kPS + lane / kL;
         const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
         const float gx = __shfl_sync(kFull, s.wx, j), gy = __shfl_sync(kFull, s.wy, j),
                     gz = __shfl_sync(kFull, s.wz, j);
         const bool gok = __shfl_sync(kFull, s.valid, j);
         float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (gok) {
-            const float4 v000 = Store<S>::quad(p.data, vb, q), v001 = Store<S>::quad(p.data, vb + 1, q);
-            const float4 v010 = Store<S>::quad(p.data, vb + sy, q), v011 = Store<S>::quad(p.data, vb + sy + 1, q);
-            const float4 v100 = Store<S>::quad(p.data, vb + sz, q), v101 = Store<S>::quad(p.data, vb + sz + 1, q);
-            const float4 v110 = Store<S>::quad(p.data, vb + sz + sy, q),
-                         v111 = Store<S>::quad(p.data, vb + sz + sy + 1, q);
+            const float4 v000 = Store<S>::quad(p.data, vb, q, kC), v001 = Store<S>::quad(p.data, vb + 1, q, kC);
+            const float4 v010 = Store<S>::quad(p.data, vb + sy, q, kC),
+                         v011 = Store<S>::quad(p.data, vb + sy + 1, q, kC);
+            const float4 v100 = Store<S>::quad(p.data, vb + sz, q, kC),
+                         v101 = Store<S>::quad(p.data, vb + sz + 1, q, kC);
+            const float4 v110 = Store<S>::quad(p.data, vb + sz + sy, q, kC),
+                         v111 = Store<S>::quad(p.data, vb + sz + sy + 1, q, kC);
             const float4 a0 = lerp4(lerp4(v000, v001, gx), lerp4(v010, v011, gx), gy);
             const float4 a1v = lerp4(lerp4(v100, v101, gx), lerp4(v110, v111, gx), gy);
             v = lerp4(a0, a1v, gz);
         }
         st4(tile + j * kRow + 4 * q, v);
-        if (to_slot) st4_keep(to_slot + j * 32 + 4 * q, v, evict_last_policy());
+        if (to_slot) st4_keep(to_slot + j * kC + 4 * q, v, evict_last_policy());
     }
     __syncwarp();
     if (s.valid) {
         // the row stays in shared memory; the shader reads the channels it needs from it
-        s.rgb = shade<kCompat>(s.nrm, d, tile + lane * kRow, &s.spec);
+        s.rgb = shade_any<kCompat, kDeg>(s.nrm, d, tile + lane * kRow, &s.spec);
     } else {
         s.rgb = f3{0.0f, 0.0f, 0.0f};
         s.spec = f3{0.0f, 0.0f, 0.0f};
@@ -270,7 +312,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t
 
 // Alpha only (no normal, gather or shading): what the backward-only pass needs to
 // rebuild the transmittance at each chunk start.  Validity matches eval_chunk.
-template <typename S>
+template <bool kCompat, typename S>
 __device__ __forceinline__ void eval_alpha(const Params &p, f3 o, f3 d, uint32_t nr, uint32_t chunk, int lane,
                                            Sample &s) {
     const uint32_t R = p.R;
@@ -302,10 +344,11 @@ __device__ __forceinline__ void eval_alpha(const Params &p, f3 o, f3 d, uint32_t
     const bool ok_prev = __shfl_up_sync(kFull, ok, 1);
     if (lane > 0) ok = ok && ok_prev;
     if (live && !cell_in_grid(to_cell(midpoint(o, d, i, p.interval), p.volume_offset, R), R)) ok = false;
+    if (!kCompat && !(isfinite(s0) && isfinite(s1))) ok = false;
     s.valid = ok;
     s.e0 = expf(-p.k * s0);
     s.e1 = expf(-p.k * s1);
-    s.alpha = ok ? fmaxf((s.e1 - s.e0) / (1.0f + s.e1), 0.0f) : 0.0f;
+    s.alpha = ok ? interval_alpha<kCompat>(s.e0, s.e1) : 0.0f;
 }
 
 // Transmittance at each lane's sample given the value at the chunk start.  kLogT uses the
@@ -352,12 +395,15 @@ struct Transmittance {
 
 // Scatter the data-gradient tile (rows of 32 channels per lane's sample) through the
 // trilinear weights: 8 lanes per sample, one 16-byte RED per lane and corner.
+template <int kDeg>
 __device__ __forceinline__ void scatter_tile(const Params &p, const float *tile, const Sample &s, int lane) {
+    using RW = Rows<kDeg>;
+    constexpr int kC = RW::kC, kRow = RW::kStride, kL = RW::kLanes, kPS = RW::kPerStep;
     const uint32_t R1 = p.R + 1, sy = R1, sz = R1 * R1;
-    const int q = lane & 7;
+    const int q = lane % kL;
 #pragma unroll 2
-    for (int st = 0; st < 8; ++st) {
-        const int j = st * 4 + (lane >> 3);
+    for (int st = 0; st < kL; ++st) {
+        const int j = st * kPS + lane / kL;
         const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
         const float px = __shfl_sync(kFull, s.wx, j), py = __shfl_sync(kFull, s.wy, j),
                     pz = __shfl_sync(kFull, s.wz, j);
@@ -368,15 +414,15 @@ __device__ __forceinline__ void scatter_tile(const Params &p, const float *tile,
         const float dx = 1 - px, dy = 1 - py;
         const float4 a0 = scale4(g, 1 - pz), a1 = scale4(g, pz);
         const float4 a00 = scale4(a0, dy), a01 = scale4(a0, py), a10 = scale4(a1, dy), a11 = scale4(a1, py);
-        float *b = p.data_grad + 32ull * vb + 4 * q;
+        float *b = p.data_grad + (uint64_t)kC * vb + 4 * q;
         red4(b, scale4(a00, dx));
-        red4(b + 32, scale4(a00, px));
-        red4(b + 32ull * sy, scale4(a01, dx));
-        red4(b + 32ull * sy + 32, scale4(a01, px));
-        red4(b + 32ull * sz, scale4(a10, dx));
-        red4(b + 32ull * sz + 32, scale4(a10, px));
-        red4(b + 32ull * (sz + sy), scale4(a11, dx));
-        red4(b + 32ull * (sz + sy) + 32, scale4(a11, px));
+        red4(b + kC, scale4(a00, px));
+        red4(b + (uint64_t)kC * sy, scale4(a01, dx));
+        red4(b + (uint64_t)kC * sy + kC, scale4(a01, px));
+        red4(b + (uint64_t)kC * sz, scale4(a10, dx));
+        red4(b + (uint64_t)kC * sz + kC, scale4(a10, px));
+        red4(b + (uint64_t)kC * (sz + sy), scale4(a11, dx));
+        red4(b + (uint64_t)kC * (sz + sy) + kC, scale4(a11, px));
     }
 }
 
@@ -386,8 +432,10 @@ __device__ __forceinline__ void red_cell(float *g8, uint32_t cell, const float *
     red4(b + 4, make_float4(g[4], g[5], g[6], 0.0f));
 }
 
-template <bool kCompat, typename S, int kPass, bool kLogT>
+template <bool kCompat, typename S, int kPass, bool kLogT, int kDeg>
 __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kernel(const Params p) {
+    constexpr int kRow = Rows<kDeg>::kStride;
+    constexpr uint32_t kChunkFloats = chunk_floats<kDeg>();
     __shared__ __align__(16) float tiles[kWarpsPerBlock][kWarp * kRow];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     float *tile = tiles[w];
@@ -431,13 +479,13 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                         if (c < 32) ts_lo = tr.carry; else ts_hi = tr.carry;
                     }
                     if (kPass == kBackward) {
-                        eval_alpha<S>(p, o, d, nr, c, lane, s);
+                        eval_alpha<kCompat, S>(p, o, d, nr, c, lane, s);
                         tr.step(s.alpha, s.valid, lane);
                     } else {
                         float *stash = (slot && c + 1 < chunks && c + 1 + kSlotChunks >= chunks)
                                            ? slot + (c % kSlotChunks) * kChunkFloats
                                            : nullptr;
-                        eval_chunk<kCompat, S>(p, o, d, nr, c, lane, tile, s, nullptr, stash);
+                        eval_chunk<kCompat, S, kDeg>(p, o, d, nr, c, lane, tile, s, nullptr, stash);
                         const float T = tr.step(s.alpha, s.valid, lane);
                         T_last = T;
                         acc.x += s.rgb.x * s.alpha * T;
@@ -476,7 +524,7 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                     const float *stashed = (slot && (uint32_t)c + 1 + kSlotChunks >= chunks)
                                                ? slot + ((uint32_t)c % kSlotChunks) * kChunkFloats
                                                : nullptr;
-                    eval_chunk<kCompat, S>(p, o, d, nr, (uint32_t)c, lane, tile, s, stashed);
+                    eval_chunk<kCompat, S, kDeg>(p, o, d, nr, (uint32_t)c, lane, tile, s, stashed);
                     T = tr.step(s.alpha, s.valid, lane);
                 }
                 const float a = s.alpha;
@@ -533,11 +581,7 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                 }
                 // dalpha/dsdf (kernel/render.cu:271-278), zero where alpha == 0
                 float d_this = 0.0f, d_next = 0.0f;
-                if (s.valid && a != 0.0f) {
-                    const float inv = 1.0f / (1.0f + s.e1);
-                    d_next = -p.k * s.e1 * (1.0f + s.e0) * inv * inv;
-                    d_this = p.k * s.e0 * inv;
-                }
+                if (s.valid && a != 0.0f) interval_dalpha<kCompat>(s.e0, s.e1, p.k, &d_next, &d_this);
                 const float mine_this = dl * d_this;
                 float from_next = __shfl_down_sync(kFull, mine_this, 1);
                 if (lane == kWarp - 1) from_next = next_this;
@@ -551,7 +595,7 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                     // rgb gradient -> shader backward (data gradient into the tile, normal gradient)
                     const f3 grgb{g.x * T * a, g.y * T * a, g.z * T * a};
                     // data gradient written over the data row (every read precedes its write)
-                    const f3 gn = shade_backward_inplace<kCompat>(grgb, s.nrm, d, tile + lane * kRow, s.spec);
+                    const f3 gn = shade_any_backward_inplace<kCompat, kDeg>(grgb, s.nrm, d, tile + lane * kRow, s.spec);
                     float ar[7], gr[6];
                     Store<S>::cell(p.sdf, (uint32_t)s.cr.index, ar);
                     quad_normal_grad(ar, s.cr.u, gn, gr);
@@ -573,7 +617,7 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                     }
                 }
                 __syncwarp();
-                scatter_tile(p, tile, s, lane);
+                scatter_tile<kDeg>(p, tile, s, lane);
                 __syncwarp();
             }
         }
@@ -585,6 +629,27 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
 
 constexpr size_t kCounterBytes = 256;
 
+// Calls f.template run<kCompat, S, kLogT, kDeg>() for the kernel configuration of `a`
+// (degree 3 exists only in the packed, fixed-mode layout).
+template <typename F>
+void dispatch(const qsdvr_render_args *a, F &f) {
+    const bool compat = a->mode == QSDVR_MODE_COMPAT;
+    const bool bf16 = a->storage == QSDVR_STORAGE_BF16;
+    const bool logt = a->transmittance == QSDVR_TRANSMITTANCE_LOG;
+    const bool deg3 = a->sh_degree == 3;
+    using B = __nv_bfloat16;
+    if (deg3) {
+        if (bf16) { if (logt) f.template run<false, B, true, 3>(); else f.template run<false, B, false, 3>(); }
+        else { if (logt) f.template run<false, float, true, 3>(); else f.template run<false, float, false, 3>(); }
+    } else if (compat) {
+        if (bf16) { if (logt) f.template run<true, B, true, 2>(); else f.template run<true, B, false, 2>(); }
+        else { if (logt) f.template run<true, float, true, 2>(); else f.template run<true, float, false, 2>(); }
+    } else {
+        if (bf16) { if (logt) f.template run<false, B, true, 2>(); else f.template run<false, B, false, 2>(); }
+        else { if (logt) f.template run<false, float, true, 2>(); else f.template run<false, float, false, 2>(); }
+    }
+}
+
 // Persistent grid and workspace size for the current device: one block per resident slot
 // of the train kernel (the heaviest instantiation, which bounds the others).
 struct Layout {
@@ -593,36 +658,46 @@ struct Layout {
     size_t counter_bytes, train_bytes;
 };
 
+struct Occupancy {
+    int per_sm = 0;
+    size_t chunk_bytes = 0;
+    cudaError_t err = cudaSuccess;
+    template <bool C, typename S, bool L, int D>
+    void run() {
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<C, S, kTrain, L, D>, kThreads, 0);
+        chunk_bytes = chunk_floats<D>() * sizeof(float);
+    }
+};
+
 Layout layout_for(const qsdvr_render_args *a) {
     Layout L{QSDVR_OK, 0, kCounterBytes, 0};
-    int dev = 0, sms = 0, per_sm = 0;
+    int dev = 0, sms = 0;
     if (check_cuda(cudaGetDevice(&dev), "render: cudaGetDevice") != QSDVR_OK ||
         check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "render: SM count") != QSDVR_OK) {
         L.error = QSDVR_ERR_CUDA;
         return L;
     }
-    const bool compat = a->mode == QSDVR_MODE_COMPAT;
-    const bool bf16 = a->storage == QSDVR_STORAGE_BF16;
-    const bool logt = a->transmittance == QSDVR_TRANSMITTANCE_LOG;
-    const void *fn;
-#define QSDVR_FN(C, S, L2) fn = reinterpret_cast<const void *>(&render_kernel<C, S, kTrain, L2>)
-    if (compat) {
-        if (bf16) { if (logt) QSDVR_FN(true, __nv_bfloat16, true); else QSDVR_FN(true, __nv_bfloat16, false); }
-        else { if (logt) QSDVR_FN(true, float, true); else QSDVR_FN(true, float, false); }
-    } else {
-        if (bf16) { if (logt) QSDVR_FN(false, __nv_bfloat16, true); else QSDVR_FN(false, __nv_bfloat16, false); }
-        else { if (logt) QSDVR_FN(false, float, true); else QSDVR_FN(false, float, false); }
-    }
-#undef QSDVR_FN
-    if (check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0), "render: occupancy") !=
-        QSDVR_OK) {
+    Occupancy occ;
+    dispatch(a, occ);
+    if (check_cuda(occ.err, "render: occupancy") != QSDVR_OK) {
         L.error = QSDVR_ERR_CUDA;
         return L;
     }
-    L.blocks = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
-    L.train_bytes = kCounterBytes + (size_t)L.blocks * kWarpsPerBlock * kSlotChunks * kChunkFloats * sizeof(float);
+    L.blocks = (unsigned)(sms * (occ.per_sm > 0 ? occ.per_sm : 1));
+    L.train_bytes = kCounterBytes + (size_t)L.blocks * kWarpsPerBlock * kSlotChunks * occ.chunk_bytes;
     return L;
 }
+
+template <int kPass>
+struct Launcher {
+    const Params *p;
+    unsigned blocks;
+    cudaStream_t stream;
+    template <bool C, typename S, bool L, int D>
+    void run() {
+        render_kernel<C, S, kPass, L, D><<<blocks, kThreads, 0, stream>>>(*p);
+    }
+};
 
 template <int kPass>
 int launch(const qsdvr_render_args *a, cudaStream_t stream) {
@@ -659,18 +734,8 @@ int launch(const qsdvr_render_args *a, cudaStream_t stream) {
         if (st != QSDVR_OK) return st;
         blocks = L.blocks;
     }
-    const bool compat = a->mode == QSDVR_MODE_COMPAT;
-    const bool bf16 = a->storage == QSDVR_STORAGE_BF16;
-    const bool logt = a->transmittance == QSDVR_TRANSMITTANCE_LOG;
-#define QSDVR_LAUNCH(C, S, L) render_kernel<C, S, kPass, L><<<blocks, kThreads, 0, stream>>>(p)
-    if (compat) {
-        if (bf16) { if (logt) QSDVR_LAUNCH(true, __nv_bfloat16, true); else QSDVR_LAUNCH(true, __nv_bfloat16, false); }
-        else { if (logt) QSDVR_LAUNCH(true, float, true); else QSDVR_LAUNCH(true, float, false); }
-    } else {
-        if (bf16) { if (logt) QSDVR_LAUNCH(false, __nv_bfloat16, true); else QSDVR_LAUNCH(false, __nv_bfloat16, false); }
-        else { if (logt) QSDVR_LAUNCH(false, float, true); else QSDVR_LAUNCH(false, float, false); }
-    }
-#undef QSDVR_LAUNCH
+    Launcher<kPass> launcher{&p, blocks, stream};
+    dispatch(a, launcher);
     return check_launch(kPass == kForward ? "qsdvr_render_forward"
                                           : (kPass == kBackward ? "qsdvr_render_backward" : "qsdvr_render_train"));
 }
@@ -685,6 +750,10 @@ int validate(const qsdvr_render_args *a, int pass) {
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: bad mode %d", a->mode);
     if (a->storage != QSDVR_STORAGE_F32 && a->storage != QSDVR_STORAGE_BF16)
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: bad storage %d", a->storage);
+    if (a->sh_degree != 0 && a->sh_degree != 2 && a->sh_degree != 3)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: sh_degree %d not supported (2 or 3)", a->sh_degree);
+    if (a->sh_degree == 3 && a->mode == QSDVR_MODE_COMPAT)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: SH degree 3 exists only in fixed mode");
     if (a->transmittance != QSDVR_TRANSMITTANCE_PRODUCT && a->transmittance != QSDVR_TRANSMITTANCE_LOG)
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: bad transmittance form %d", a->transmittance);
     if (!(a->interval > 0.0f)) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: interval must be > 0");

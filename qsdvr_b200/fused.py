@@ -28,7 +28,7 @@ MODES = {"compat": _lib.MODE_COMPAT, "fixed": _lib.MODE_FIXED}
 class RenderArgs(ctypes.Structure):
     """qsdvr_render_args (include/qsdvr_b200.h)."""
     _fields_ = [("rays", P), ("origin", P), ("dir", P), ("ray_count", U32), ("reso", U32), ("interval", F32),
-                ("logistic_coef", F32), ("mode", I32), ("storage", I32), ("transmittance", I32), ("reserved", I32),
+                ("logistic_coef", F32), ("mode", I32), ("storage", I32), ("transmittance", I32), ("sh_degree", I32),
                 ("sdf_grid", P), ("data", P), ("color", P), ("target", P), ("grad_color", P), ("sdf_grad", P),
                 ("data_grad", P), ("loss", P), ("grad_scale", F32), ("workspace", P), ("workspace_bytes", ctypes.c_uint64)]
 
@@ -45,7 +45,7 @@ _workspaces: dict = {}
 def workspace(device, args: "RenderArgs") -> torch.Tensor:
     """A cached workspace for the persistent kernels on ``device`` (one per device and
     kernel configuration; launches on one stream never overlap, so it can be reused)."""
-    key = (device, args.mode, args.storage, args.transmittance)
+    key = (device, args.mode, args.storage, args.transmittance, args.sh_degree)
     need = int(_lib.lib().qsdvr_render_workspace_size(ctypes.byref(args)))
     ws = _workspaces.get(key)
     if ws is None or ws.numel() < need:
@@ -71,11 +71,21 @@ def _check_batch(rays, origin, direction):
     return dev, n
 
 
+def sh_degree_of(data, R) -> int:
+    """SH degree implied by the appearance grid: 32-channel rows are degree 2 (the
+    reference), 64-channel rows degree 3."""
+    c = data.numel() // (R + 1) ** 3
+    if c * (R + 1) ** 3 != data.numel() or c not in (32, 64):
+        raise ValueError(f"data must be [(R+1)^3, 32] or [(R+1)^3, 64] for R={R}")
+    return 2 if c == 32 else 3
+
+
 def _grid_storage(sdf_grid, data, R):
     if sdf_grid.dtype != data.dtype or sdf_grid.dtype not in (torch.float32, torch.bfloat16):
         raise TypeError("sdf_grid and data must both be float32 or both bfloat16")
-    if sdf_grid.numel() != 8 * R ** 3 or data.numel() != 32 * (R + 1) ** 3:
-        raise ValueError(f"sdf_grid must be [R^3,8] and data [(R+1)^3,32] for R={R}")
+    if sdf_grid.numel() != 8 * R ** 3:
+        raise ValueError(f"sdf_grid must be [R^3,8] for R={R}")
+    sh_degree_of(data, R)
     if not (sdf_grid.is_contiguous() and data.is_contiguous()):
         raise ValueError("grids must be contiguous")
     return STORAGE["bf16" if sdf_grid.dtype == torch.bfloat16 else "f32"]
@@ -92,6 +102,7 @@ def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="
     a.mode = MODES[mode]
     a.storage = _grid_storage(sdf_grid, data, int(reso))
     a.transmittance = TRANSMITTANCE[transmittance]
+    a.sh_degree = sh_degree_of(data, int(reso))
     a.sdf_grid, a.data = _ptr(sdf_grid), _ptr(data)
     a.color, a.target, a.grad_color = _ptr(color), _ptr(target), _ptr(grad_color)
     a.sdf_grad, a.data_grad, a.loss = _ptr(sdf_grad), _ptr(data_grad), _ptr(loss)

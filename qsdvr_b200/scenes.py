@@ -132,16 +132,20 @@ def procedural_grid(R: int, seed: int = 0, device="cpu", chunk: int = 64) -> tor
 
 # ----------------------------------------------------------------------------- appearance
 
-def appearance(R: int, seed: int = 0, device="cpu", procedural: bool = False) -> torch.Tensor:
-    """[(R+1)^3, 32] vertex data (vertex x + y(R+1) + z(R+1)^2), packed SH order."""
+def appearance(R: int, seed: int = 0, device="cpu", procedural: bool = False, sh_degree: int = 2) -> torch.Tensor:
+    """[(R+1)^3, C] vertex data (vertex x + y(R+1) + z(R+1)^2), packed SH order.
+    Degree 2: C = 32 (27 SH, diffuse 27..29, metallic 30, ao 31), the reference's layout;
+    degree 3: C = 64 (48 SH, diffuse 48..50, metallic 51, ao 52, 53..63 zero)."""
     V = (R + 1) ** 3
+    nsh = 3 * (sh_degree + 1) ** 2
+    C = 32 if sh_degree == 2 else 64
     gen = torch.Generator(device=device).manual_seed(seed)
-    d = torch.empty((V, 32), dtype=torch.float32, device=device)
+    d = torch.zeros((V, C), dtype=torch.float32, device=device)
     d[:, 0:3] = 0.5 + 0.05 * torch.randn((V, 3), generator=gen, device=device)
-    d[:, 3:27] = 0.1 * torch.randn((V, 24), generator=gen, device=device)
-    d[:, 27:30] = torch.rand((V, 3), generator=gen, device=device)
-    d[:, 30] = torch.rand(V, generator=gen, device=device)
-    d[:, 31] = 0.5 + 0.5 * torch.rand(V, generator=gen, device=device)
+    d[:, 3:nsh] = 0.1 * torch.randn((V, nsh - 3), generator=gen, device=device)
+    d[:, nsh:nsh + 3] = torch.rand((V, 3), generator=gen, device=device)
+    d[:, nsh + 3] = torch.rand(V, generator=gen, device=device)
+    d[:, nsh + 4] = 0.5 + 0.5 * torch.rand(V, generator=gen, device=device)
     if procedural:
         # smooth seeded RGB field projected onto the DC coefficient and the diffuse colour
         n = torch.arange(R + 1, device=device, dtype=torch.float32) * (2.0 / R) - 1.0
@@ -154,5 +158,5 @@ def appearance(R: int, seed: int = 0, device="cpu", procedural: bool = False) ->
             rgb = 0.5 + 0.45 * torch.sin(p @ f.T + ph)
             lo, hi = z0 * (R + 1) ** 2, min(R + 1, z0 + 32) * (R + 1) ** 2
             d[lo:hi, 0:3] = rgb / (2 * 0.28209479177387814)
-            d[lo:hi, 27:30] = rgb
+            d[lo:hi, nsh:nsh + 3] = rgb
     return d

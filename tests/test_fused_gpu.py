@@ -215,3 +215,31 @@ def test_persistent_stash_path_matches_one_ray_per_block(fz, mode):
     assert (c0 - c1).abs().max().item() < 1e-6
     assert abs(l0.item() - l1.item()) < 1e-5 * max(1.0, l0.item())
     assert rel_err(s1.cpu(), s0.cpu()) < 1e-5 and rel_err(d1.cpu(), d0.cpu()) < 1e-5
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+def test_fused_sh_degree3_vs_oracle(fz, storage):
+    """SH degree 3 (64-channel rows, fixed mode): forward and gradients against the float64
+    oracle with autograd."""
+    from qsdvr_b200 import scenes
+
+    R, k, interval = 24, 8.0, 4.0 / 160
+    cam = camera_batch((-1.9, 3.2, 1.4), 40, 55.0, interval, R)
+    grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.55, 0.01, seed=21).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=21, sh_degree=3).to(DEV)
+    if storage == "bf16":
+        grid8, data = grid8.to(torch.bfloat16).float(), data.to(torch.bfloat16).float()
+    gk, dk = (grid8.to(torch.bfloat16), data.to(torch.bfloat16)) if storage == "bf16" else (grid8, data)
+    target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(22)).to(DEV)
+    sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+    img, _ = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, gk, dk, R, interval, k, sg, dg,
+                             mode="fixed", transmittance="log" if storage == "bf16" else "product")
+    g7 = grid8[:, :7].double().cpu().requires_grad_()
+    dd = data.double().cpu().requires_grad_()
+    want = O.render(g7, dd, oracle_inputs(cam), k, compat=False, sh_degree=3)
+    loss = ((want - target.double().cpu()) ** 2).mean()
+    wg, wd = torch.autograd.grad(loss, (g7, dd))
+    assert (img.cpu().double() - want.detach()).abs().max().item() < IMG_TOL
+    assert rel_err(sg[:, :7].cpu(), wg) < GRAD_TOL
+    assert rel_err(dg.cpu(), wd) < GRAD_TOL
+    assert float(dg[:, 53:].abs().max()) == 0.0  # unused channels get no gradient
