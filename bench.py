@@ -316,7 +316,7 @@ def run_ours(args, cfg, device, ws, rank):
     alg_bytes = mean_samples * bps + cfg["rays"] * BYTES_PER_RAY
     achieved = alg_bytes / (kern_avg / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    tps = profiled_traffic_per_sample(storage)
+    tps = profiled_traffic_per_sample(storage + ("_sh3" if cfg.get("sh", 2) == 3 else ""))
     traffic = None if tps is None else tps * mean_samples
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "rays/s", "n_gpus": ws, "steps": args.steps,
