@@ -39,7 +39,8 @@ enum {
 enum {
     QSDVR_DEVERR_INDEX = 1u,        /* a cell / vertex index outside the grid         */
     QSDVR_DEVERR_CAPACITY = 2u,     /* a ray's samples run past the sample buffers     */
-    QSDVR_DEVERR_RAY = 4u           /* a ray record is inconsistent (count 1, overflow) */
+    QSDVR_DEVERR_RAY = 4u,          /* a ray record is inconsistent (count 1, overflow) */
+    QSDVR_DEVERR_TIMEOUT = 8u       /* a bounded wait on the tensor cores gave up       */
 };
 
 /* Shading / indexing modes. */
@@ -224,6 +225,12 @@ typedef struct qsdvr_render_args {
     float grad_scale;         /* train: dL/dcolor = grad_scale * (color - target) */
     void *workspace;          /* optional, 256-byte aligned: enables the persistent grid with     */
     uint64_t workspace_bytes; /* dynamic ray scheduling and, in train, the per-warp row stash    */
+    const float *tlist;       /* optional [ray_count][33]: SDF sample positions t (from origin) of
+                                 each ray, replacing the uniform march (32 render samples at the
+                                 interval midpoints); rays with sdf_count < 2 stay empty          */
+    float *sample_alpha;      /* optional: alpha of render sample i of ray r written at
+                                 rays[r].render_offset + i (forward and train)                   */
+    uint64_t sample_capacity; /* length of sample_alpha */
 } qsdvr_render_args;
 
 /* Workspace bytes for qsdvr_render_* with these args on the current device (mode, storage
@@ -279,6 +286,36 @@ int qsdvr_adam_step(const qsdvr_adam_args *args, cudaStream_t stream);
 int qsdvr_render_loss_f64(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
                           uint32_t reso, float interval, double logistic_coef, const double *sdf_grid,
                           const double *data, const double *target, double *loss_per_ray, cudaStream_t stream);
+
+/* ---- proposal network (no counterpart in the reference) ----------------------------------
+ * A 32-d positional encoding -> 64 -> 64 -> 1 MLP bounding the renderer's density; BF16
+ * weights (params_bf16: QSDVR_MLP_PARAMS values, layout in qsdvr_b200/csrc/proposal.cu),
+ * FP32 accumulation on the tcgen05 tensor cores. */
+#define QSDVR_MLP_PARAMS 6280
+
+/* Density bound at points [count][4] (x, y, z, ignored), or, when rays is not null, at the
+ * 64 coarse points t = (j + 0.5) L / 64 of every ray (L = (sdf_count - 1) interval); out is
+ * [count] or [ray_count][64]. */
+int qsdvr_mlp_density(const float *points, uint32_t count, const qsdvr_ray_info *rays, const float *origin,
+                      const float *dir, uint32_t ray_count, float interval, const void *params_bf16, float *out,
+                      cudaStream_t stream);
+
+/* One training pass over points [count][4] (x, y, z, target density): accumulates the
+ * gradient of mean_p w (log1p(bound) - log1p(target))^2 (w = under_weight where the bound is
+ * below the target) into grad [QSDVR_MLP_PARAMS] fp32 and the loss into *loss. */
+int qsdvr_mlp_train(const float *points, uint32_t count, const void *params_bf16, float under_weight, float *grad,
+                    float *loss, cudaStream_t stream);
+
+/* Fine sample positions [ray_count][33] from the coarse densities [ray_count][64]: inverse
+ * CDF of the coarse compositing weights (mixed with 5% uniform) at quantiles k/32. */
+int qsdvr_proposal_sample(const qsdvr_ray_info *rays, uint32_t ray_count, float interval, const float *coarse_density,
+                          float *tlist, cudaStream_t stream);
+
+/* Training points for the proposal network from a uniform-march forward: render sample i
+ * of ray r at rays[r].render_offset + i gets (position, -log(1 - alpha) / interval). */
+int qsdvr_proposal_targets(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
+                           float interval, const float *alpha, uint64_t sample_count, float *points,
+                           cudaStream_t stream);
 
 #ifdef __cplusplus
 }

@@ -84,6 +84,7 @@ def _lib():
         lib.oracle_ray_cut.argtypes = [ctypes.POINTER(_Camera), P, ctypes.c_uint32, ctypes.c_float, P, P, P, P]
         lib.oracle_generate_ray_points.argtypes = [P, P, P, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32,
                                                    P, P, P, P, P]
+        lib.oracle_list_points.argtypes = [P, P, P, ctypes.c_uint32, P, ctypes.c_uint32, P, P, P, P, P]
         _raygen = lib
     return _raygen
 
@@ -151,6 +152,33 @@ def generate_ray_points(rays: np.ndarray, origin: np.ndarray, direction: np.ndar
                                       _ptr(out["sdfPointList"]), _ptr(out["sdfIndexList"]),
                                       _ptr(out["renderPointList"]), _ptr(out["renderIndexList"]),
                                       _ptr(out["viewDirList"]))
+    return out
+
+
+def list_points(rays: np.ndarray, origin: np.ndarray, direction: np.ndarray, tlist: np.ndarray, reso: int):
+    """Sample lists of the fused renderer's list sampling (33 SDF positions per ray from
+    ``tlist``, 32 render samples at their midpoints; raygen.c oracle_list_points), with the
+    matching ``rayList`` (rays with sdf_count < 2 keep no samples)."""
+    rays = np.ascontiguousarray(rays.astype(np.uint32))
+    origin = np.ascontiguousarray(origin.astype(np.float32))
+    direction = np.ascontiguousarray(direction.astype(np.float32))
+    tlist = np.ascontiguousarray(tlist.astype(np.float32))
+    n = rays.shape[0]
+    hit = rays[:, 0] >= 2
+    k = int(hit.sum())
+    out = dict(sdfPointList=np.zeros((33 * k, 3), np.float32), sdfIndexList=np.zeros(33 * k, np.int32),
+               renderPointList=np.zeros((32 * k, 3), np.float32), renderIndexList=np.zeros(32 * k, np.int32),
+               viewDirList=np.zeros((32 * k, 3), np.float32))
+    _lib().oracle_list_points(_ptr(rays), _ptr(origin), _ptr(direction), n, _ptr(tlist), reso,
+                              _ptr(out["sdfPointList"]), _ptr(out["sdfIndexList"]), _ptr(out["renderPointList"]),
+                              _ptr(out["renderIndexList"]), _ptr(out["viewDirList"]))
+    rank = np.cumsum(hit) - hit
+    rl = np.zeros((n, 4), np.int32)
+    rl[hit, 0] = 33
+    rl[hit, 1] = 33 * rank[hit]
+    rl[hit, 2] = 32
+    rl[hit, 3] = 32 * rank[hit]
+    out["rayList"] = rl
     return out
 
 

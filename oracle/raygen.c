@@ -148,3 +148,36 @@ void oracle_generate_ray_points(const uint32_t *rays, const float *origin, const
         }
     }
 }
+
+/*
+ * List sampling (the proposal path of the fused renderer; no reference counterpart): ray r
+ * with sdf_count >= 2 gets the 33 SDF samples fmaf(d, t_j, o) for t_j = tlist[33 r + j] and
+ * the 32 render samples at 0.5 (t_j + t_{j+1}), converted to cells like camera.cu:73-80.
+ * Outputs are packed 33 / 32 per such ray in ray order; rays with fewer samples get none.
+ */
+void oracle_list_points(const uint32_t *rays, const float *origin, const float *dir, uint32_t nrays,
+                        const float *tlist, uint32_t reso, float *sdf_pts, int32_t *sdf_idx, float *render_pts,
+                        int32_t *render_idx, float *view_dir)
+{
+    const float volume_offset = (float)reso / 2.0f;
+    size_t k = 0;
+    for (uint32_t r = 0; r < nrays; ++r) {
+        if (rays[4 * r] < 2) continue;
+        const float *o = origin + 3 * r;
+        const float *d = dir + 3 * r;
+        const float *t = tlist + 33 * (size_t)r;
+        for (uint32_t j = 0; j < 33; ++j) {
+            float p[3];
+            for (int c = 0; c < 3; ++c) p[c] = fmaf(d[c], t[j], o[c]);
+            to_cell(p, volume_offset, reso, sdf_pts + 3 * (33 * k + j), sdf_idx + 33 * k + j);
+        }
+        for (uint32_t j = 0; j < 32; ++j) {
+            const float s = 0.5f * (t[j] + t[j + 1]);
+            float p[3];
+            for (int c = 0; c < 3; ++c) p[c] = fmaf(d[c], s, o[c]);
+            to_cell(p, volume_offset, reso, render_pts + 3 * (32 * k + j), render_idx + 32 * k + j);
+            memcpy(view_dir + 3 * (32 * k + j), d, 3 * sizeof(float));
+        }
+        ++k;
+    }
+}

@@ -32,6 +32,7 @@ cudaError_t error_word_render(unsigned *, int, cudaStream_t);
 cudaError_t error_word_fused(unsigned *, int, cudaStream_t);
 cudaError_t error_word_optim(unsigned *, int, cudaStream_t);
 cudaError_t error_word_gradcheck(unsigned *, int, cudaStream_t);
+cudaError_t error_word_proposal(unsigned *, int, cudaStream_t);
 
 }  // namespace qsdvr
 
@@ -49,6 +50,7 @@ extern "C" int qsdvr_device_error(uint32_t *word, int clear, cudaStream_t stream
     if (e == cudaSuccess) e = error_word_fused(&w, clear, stream);
     if (e == cudaSuccess) e = error_word_optim(&w, clear, stream);
     if (e == cudaSuccess) e = error_word_gradcheck(&w, clear, stream);
+    if (e == cudaSuccess) e = error_word_proposal(&w, clear, stream);
     *word = w;
     return check_cuda(e, "qsdvr_device_error");
 }

@@ -105,7 +105,18 @@ struct Params {
     float grad_scale;
     uint32_t *ray_counter;  // persistent mode: next ray to take (zeroed before the launch)
     float *slots;           // persistent train mode: per-warp row stash, kSlotChunks chunks each
+    const float *tlist;     // list sampling: per ray kListT SDF positions (t from origin), or null
+    float *sample_alpha;    // optional per-render-sample alpha output (forward, train)
+    uint64_t sample_capacity;
 };
+
+constexpr uint32_t kListT = 33;  // list sampling: 33 SDF positions, 32 render samples per ray
+
+// SDF sample j and render sample j of ray r: the reference's uniform march, or positions
+// o + d t from the ray's list (render samples at interval midpoints).
+__device__ __forceinline__ f3 at_t(f3 o, f3 d, float t) {
+    return f3{fmaf(d.x, t, o.x), fmaf(d.y, t, o.y), fmaf(d.z, t, o.z)};
+}
 
 // ---- storage access --------------------------------------------------------------------
 
@@ -198,8 +209,8 @@ struct Sample {
 // kernel/surface.cu:54-115, kernel/render.cu:98-179, :239-244).  Leaves the sample's
 // interpolated 32 channels in the warp's tile.
 template <bool kCompat, typename S, int kDeg>
-__device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t nr, uint32_t chunk, int lane,
-                                           float *tile, Sample &s, const float *from_slot = nullptr,
+__device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3 d, uint32_t nr, uint32_t chunk,
+                                           int lane, float *tile, Sample &s, const float *from_slot = nullptr,
                                            float *to_slot = nullptr) {
     using RW = Rows<kDeg>;
     constexpr int kC = RW::kC, kRow = RW::kStride, kL = RW::kLanes, kPS = RW::kPerStep;
@@ -207,8 +218,10 @@ __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t
     const uint32_t i = chunk * kWarp + lane;
     const bool live = i < nr;
     bool ok = live;
+    const float *tl = p.tlist ? p.tlist + (uint64_t)kListT * r : nullptr;
     // SDF sample i+1 (this lane's interval end); sample i comes from the previous lane.
-    s.c1 = to_cell(march(o, d, (float)(i + 1), p.interval), p.volume_offset, R);
+    s.c1 = to_cell(tl ? at_t(o, d, live ? tl[i + 1] : 0.0f) : march(o, d, (float)(i + 1), p.interval),
+                   p.volume_offset, R);
     float a1[7];
     float s1 = 0.0f;
     if (live) {
@@ -221,7 +234,8 @@ __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t
     }
     float s0 = __shfl_up_sync(kFull, s1, 1);
     if (lane == 0 && live) {
-        const CellPoint c0 = to_cell(march(o, d, (float)i, p.interval), p.volume_offset, R);
+        const CellPoint c0 =
+            to_cell(tl ? at_t(o, d, tl[i]) : march(o, d, (float)i, p.interval), p.volume_offset, R);
         if (cell_in_grid(c0, R)) {
             float a0[7];
             Store<S>::cell(p.sdf, (uint32_t)c0.index, a0);
@@ -233,7 +247,8 @@ __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t
     const bool ok_prev = __shfl_up_sync(kFull, ok, 1);
     if (lane > 0) ok = ok && ok_prev;  // sdf_i is only valid if the previous lane's cell was
     // render sample i
-    s.cr = to_cell(midpoint(o, d, i, p.interval), p.volume_offset, R);
+    s.cr = to_cell(tl ? at_t(o, d, live ? 0.5f * (tl[i] + tl[i + 1]) : 0.0f) : midpoint(o, d, i, p.interval),
+                   p.volume_offset, R);
     float ar[7];
     if (live && cell_in_grid(s.cr, R)) {
         Store<S>::cell(p.sdf, (uint32_t)s.cr.index, ar);
@@ -313,13 +328,15 @@ __device__ __forceinline__ void eval_chunk(const Params &p, f3 o, f3 d, uint32_t
 // Alpha only (no normal, gather or shading): what the backward-only pass needs to
 // rebuild the transmittance at each chunk start.  Validity matches eval_chunk.
 template <bool kCompat, typename S>
-__device__ __forceinline__ void eval_alpha(const Params &p, f3 o, f3 d, uint32_t nr, uint32_t chunk, int lane,
-                                           Sample &s) {
+__device__ __forceinline__ void eval_alpha(const Params &p, uint32_t r, f3 o, f3 d, uint32_t nr, uint32_t chunk,
+                                           int lane, Sample &s) {
     const uint32_t R = p.R;
     const uint32_t i = chunk * kWarp + lane;
     const bool live = i < nr;
     bool ok = live;
-    const CellPoint c1 = to_cell(march(o, d, (float)(i + 1), p.interval), p.volume_offset, R);
+    const float *tl = p.tlist ? p.tlist + (uint64_t)kListT * r : nullptr;
+    const CellPoint c1 = to_cell(tl ? at_t(o, d, live ? tl[i + 1] : 0.0f) : march(o, d, (float)(i + 1), p.interval),
+                                 p.volume_offset, R);
     float s1 = 0.0f;
     if (live) {
         if (cell_in_grid(c1, R)) {
@@ -332,7 +349,8 @@ __device__ __forceinline__ void eval_alpha(const Params &p, f3 o, f3 d, uint32_t
     }
     float s0 = __shfl_up_sync(kFull, s1, 1);
     if (lane == 0 && live) {
-        const CellPoint c0 = to_cell(march(o, d, (float)i, p.interval), p.volume_offset, R);
+        const CellPoint c0 =
+            to_cell(tl ? at_t(o, d, tl[i]) : march(o, d, (float)i, p.interval), p.volume_offset, R);
         if (cell_in_grid(c0, R)) {
             float a0[7];
             Store<S>::cell(p.sdf, (uint32_t)c0.index, a0);
@@ -343,7 +361,10 @@ __device__ __forceinline__ void eval_alpha(const Params &p, f3 o, f3 d, uint32_t
     }
     const bool ok_prev = __shfl_up_sync(kFull, ok, 1);
     if (lane > 0) ok = ok && ok_prev;
-    if (live && !cell_in_grid(to_cell(midpoint(o, d, i, p.interval), p.volume_offset, R), R)) ok = false;
+    if (live && !cell_in_grid(to_cell(tl ? at_t(o, d, 0.5f * (tl[i] + tl[i + 1])) : midpoint(o, d, i, p.interval),
+                                      p.volume_offset, R),
+                              R))
+        ok = false;
     if (!kCompat && !(isfinite(s0) && isfinite(s1))) ok = false;
     s.valid = ok;
     s.e0 = expf(-p.k * s0);
@@ -457,7 +478,7 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
     {
         const qsdvr_ray_info info = p.rays[r];
         const uint32_t ns = info.sdf_count;
-        const uint32_t nr = ns > 1 ? ns - 1 : 0;
+        const uint32_t nr = ns > 1 ? (p.tlist ? kListT - 1 : ns - 1) : 0;
         const uint32_t chunks = (nr + kWarp - 1) / kWarp;
         const f3 o = load3(p.origin + 3ull * r), d = load3(p.dir + 3ull * r);
         f3 C{0.0f, 0.0f, 0.0f};
@@ -479,15 +500,20 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                         if (c < 32) ts_lo = tr.carry; else ts_hi = tr.carry;
                     }
                     if (kPass == kBackward) {
-                        eval_alpha<kCompat, S>(p, o, d, nr, c, lane, s);
+                        eval_alpha<kCompat, S>(p, r, o, d, nr, c, lane, s);
                         tr.step(s.alpha, s.valid, lane);
                     } else {
                         float *stash = (slot && c + 1 < chunks && c + 1 + kSlotChunks >= chunks)
                                            ? slot + (c % kSlotChunks) * kChunkFloats
                                            : nullptr;
-                        eval_chunk<kCompat, S, kDeg>(p, o, d, nr, c, lane, tile, s, nullptr, stash);
+                        eval_chunk<kCompat, S, kDeg>(p, r, o, d, nr, c, lane, tile, s, nullptr, stash);
                         const float T = tr.step(s.alpha, s.valid, lane);
                         T_last = T;
+                        if (p.sample_alpha && c * kWarp + lane < nr) {
+                            const uint64_t m = (uint64_t)info.render_offset + c * kWarp + lane;
+                            if (m < p.sample_capacity) p.sample_alpha[m] = s.alpha;
+                            else flag_error(QSDVR_DEVERR_CAPACITY);
+                        }
                         acc.x += s.rgb.x * s.alpha * T;
                         acc.y += s.rgb.y * s.alpha * T;
                         acc.z += s.rgb.z * s.alpha * T;
@@ -524,7 +550,7 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                     const float *stashed = (slot && (uint32_t)c + 1 + kSlotChunks >= chunks)
                                                ? slot + ((uint32_t)c % kSlotChunks) * kChunkFloats
                                                : nullptr;
-                    eval_chunk<kCompat, S, kDeg>(p, o, d, nr, (uint32_t)c, lane, tile, s, stashed);
+                    eval_chunk<kCompat, S, kDeg>(p, r, o, d, nr, (uint32_t)c, lane, tile, s, stashed);
                     T = tr.step(s.alpha, s.valid, lane);
                 }
                 const float a = s.alpha;
@@ -721,6 +747,9 @@ int launch(const qsdvr_render_args *a, cudaStream_t stream) {
     p.grad_scale = a->grad_scale;
     p.ray_counter = nullptr;
     p.slots = nullptr;
+    p.tlist = a->tlist;
+    p.sample_alpha = a->sample_alpha;
+    p.sample_capacity = a->sample_capacity;
     unsigned blocks = grid_for(a->ray_count, kWarpsPerBlock);
     if (a->workspace) {
         const Layout L = layout_for(a);

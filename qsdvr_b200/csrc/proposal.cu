@@ -1,0 +1,603 @@
+// Proposal network: a small MLP (32-d positional encoding -> 64 -> 64 -> 1, BF16 weights,
+// FP32 accumulation) that bounds the renderer's density so that 32 fine samples per ray,
+// placed by inverse-CDF sampling of 64 coarse MLP evaluations, replace the uniform march.
+// No counterpart in the reference.
+//
+// GEMMs run on the 5th-generation tensor cores (tcgen05): a CTA of 128 threads owns a tile of
+// 128 points (thread t <-> point t <-> TMEM lane t); operands are staged in shared memory in
+// canonical no-swizzle layouts, one thread issues the MMAs, accumulators live in TMEM.  The
+// training kernel keeps the weight-gradient accumulators in TMEM across all of its tiles.
+//
+// Parameter vector (fp32 master, bf16 copy read by the kernels), QSDVR_MLP_PARAMS floats:
+//   [0, 2048)    W1[o][i], 64 x 32 (input feature 27 is the constant 1: the layer-1 bias)
+//   [2048, 6144) W2[o][i], 64 x 64
+//   [6144, 6208) b2[64]   [6208, 6272) w3[64]   [6272] b3   (padded to 6280)
+// Encoding of p in [-1,1]^3: f0..2 = p, f(3 + 6l + 2c) = sin(pi 2^l p_c), f(4 + 6l + 2c) =
+// cos(pi 2^l p_c) for l = 0..3, f27 = 1, f28..31 = 0.  Density bound = softplus(w3 . h2 + b3).
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "raygen.cuh"
+#include "tcgen05.cuh"
+
+namespace qsdvr {
+
+QSDVR_ERROR_WORD_ACCESSOR(proposal)
+
+namespace {
+
+constexpr int kTile = 128;
+constexpr int kF = 32, kH = 64;
+constexpr int kOffW2 = 2048, kOffB2 = 6144, kOffW3 = 6208, kOffB3 = 6272;
+constexpr uint32_t kSpins = 1u << 26;  // bounded mbarrier waits (~ seconds), then give up
+
+// shared-memory operand layouts (bytes): element (row, feature) of an activation buffer with
+// point-group stride SP sits at (row/8)*SP + (f/8)*128 + (row%8)*16 + (f%8)*2
+constexpr uint32_t kSpX = 512, kSpH = 1024, kSpG = 2048;  // X (32 f), H1 (64 f), grads (64 f + 64 zero)
+constexpr uint32_t kBytesX = 16 * kSpX, kBytesH = 16 * kSpH, kBytesG = 16 * kSpG;
+constexpr uint32_t kBytesW1 = 8 * 512, kBytesW2 = 8 * 1024;
+
+__device__ __forceinline__ uint32_t act_off(uint32_t row, uint32_t f, uint32_t sp) {
+    return (row >> 3) * sp + (f >> 3) * 128 + (row & 7) * 16 + (f & 7) * 2;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__device__ __forceinline__ float bf16f(const __nv_bfloat16 *p, int i) { return __bfloat162float(p[i]); }
+
+// Write 8 consecutive features [8g, 8g+8) of one row as one 16-byte store.
+__device__ __forceinline__ void store_row8(uint8_t *buf, uint32_t row, uint32_t g, uint32_t sp, const float *v) {
+    uint4 q;
+    q.x = pack_bf16(v[0], v[1]);
+    q.y = pack_bf16(v[2], v[3]);
+    q.z = pack_bf16(v[4], v[5]);
+    q.w = pack_bf16(v[6], v[7]);
+    *reinterpret_cast<uint4 *>(buf + act_off(row, 8 * g, sp)) = q;
+}
+
+__device__ __forceinline__ void encode(f3 p, float *f) {
+    f[0] = p.x;
+    f[1] = p.y;
+    f[2] = p.z;
+    const float c[3] = {p.x, p.y, p.z};
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float s, co;
+            sincospif(c[k] * (float)(1 << l), &s, &co);
+            f[3 + 6 * l + 2 * k] = s;
+            f[4 + 6 * l + 2 * k] = co;
+        }
+    }
+    f[27] = 1.0f;
+    f[28] = f[29] = f[30] = f[31] = 0.0f;
+}
+
+__device__ __forceinline__ float softplus(float y) { return y > 20.0f ? y : log1pf(expf(y)); }
+__device__ __forceinline__ float sigmoid(float y) { return 1.0f / (1.0f + expf(-y)); }
+
+// Stage W1 / W2 (bf16) in their canonical K-major layouts: element (o, i) at
+// (o/8)*SO + (i/8)*128 + (o%8)*16 + (i%8)*2 with SO = 512 (W1) or 1024 (W2).
+__device__ void stage_weights(const __nv_bfloat16 *w, uint8_t *w1s, uint8_t *w2s) {
+    for (int idx = threadIdx.x; idx < 64 * 4; idx += blockDim.x) {  // W1: 64 rows x 4 groups
+        const int o = idx >> 2, g = idx & 3;
+        *reinterpret_cast<uint4 *>(w1s + act_off(o, 8 * g, 512)) = *reinterpret_cast<const uint4 *>(w + o * 32 + 8 * g);
+    }
+    for (int idx = threadIdx.x; idx < 64 * 8; idx += blockDim.x) {  // W2: 64 rows x 8 groups
+        const int o = idx >> 3, g = idx & 7;
+        *reinterpret_cast<uint4 *>(w2s + act_off(o, 8 * g, 1024)) =
+            *reinterpret_cast<const uint4 *>(w + kOffW2 + o * 64 + 8 * g);
+    }
+}
+
+struct Sync {
+    uint64_t *mbar;
+    uint32_t phase;
+    bool ok;
+    // commit the MMAs issued by thread 0 and wait for them on every thread; a wait that gave
+    // up stops the whole CTA (the flag is made block-uniform so every thread leaves the tile
+    // loop at the same barrier)
+    __device__ __forceinline__ void complete() {
+        if (threadIdx.x == 0) tc::commit(mbar);
+        const bool done = tc::mbar_wait(mbar, phase, kSpins);
+        if (!done) flag_error(QSDVR_DEVERR_TIMEOUT);
+        if (__syncthreads_or(!done)) ok = false;
+        phase ^= 1u;
+        tc::fence_after_sync();
+    }
+};
+
+// smem staging -> visible to the tensor core, and everyone past their TMEM reads
+__device__ __forceinline__ void handoff() {
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+}
+
+// Forward of one tile: X (staged) -> H1 (staged, returns relu mask) -> z2 = W2 h1 + b2 (row in registers).
+__device__ __forceinline__ uint64_t forward_tile(uint8_t *xs, uint8_t *hs, uint8_t *w1s, uint8_t *w2s, uint32_t tmem,
+                                                 Sync &sync, const float *b2, float *z2) {
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+    constexpr uint32_t i1 = tc::idesc_bf16(128, 64, false, false);
+    handoff();
+    if (t == 0) {
+        for (int s = 0; s < 2; ++s)
+            tc::mma_bf16(tmem + 0, tc::smem_desc(tc::smem_addr(xs) + 256 * s, 128, kSpX),
+                         tc::smem_desc(tc::smem_addr(w1s) + 256 * s, 128, 512), i1, s > 0);
+    }
+    sync.complete();
+    uint64_t mask = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float v[16];
+        tc::tmem_ld16(tc::tmem_at(tmem, 32 * warp, 16 * j), v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            if (v[q] > 0.0f) mask |= 1ull << (16 * j + q);
+            v[q] = fmaxf(v[q], 0.0f);
+        }
+        store_row8(hs, t, 2 * j, kSpH, v);
+        store_row8(hs, t, 2 * j + 1, kSpH, v + 8);
+    }
+    handoff();
+    if (t == 0) {
+        for (int s = 0; s < 4; ++s)
+            tc::mma_bf16(tmem + 64, tc::smem_desc(tc::smem_addr(hs) + 256 * s, 128, kSpH),
+                         tc::smem_desc(tc::smem_addr(w2s) + 256 * s, 128, 1024), i1, s > 0);
+    }
+    sync.complete();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float v[16];
+        tc::tmem_ld16(tc::tmem_at(tmem, 32 * warp, 64 + 16 * j), v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) z2[16 * j + q] = v[q] + b2[16 * j + q];
+    }
+    return mask;
+}
+
+// ---- training -------------------------------------------------------------------------------
+
+struct TrainSmem {
+    float b2[64], w3[64], db2[64], dw3[64], db3, loss;
+    uint64_t mbar;
+    uint32_t tmem;
+};
+
+// points [P][4] = (x, y, z, target density).  Loss per point (mean over P):
+// w (log1p(s) - log1p(t))^2 with s = softplus(y) the bound and w = under_weight when s < t.
+__global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict__ pts, uint32_t P,
+                                                        const __nv_bfloat16 *__restrict__ w, float under_weight,
+                                                        float *__restrict__ grad, float *__restrict__ loss_out) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *xs = smem;
+    uint8_t *hs = xs + kBytesX;
+    uint8_t *g2 = hs + kBytesH;
+    uint8_t *g1 = g2 + kBytesG;
+    uint8_t *w1s = g1 + kBytesG;
+    uint8_t *w2s = w1s + kBytesW1;
+    TrainSmem &S = *reinterpret_cast<TrainSmem *>(w2s + kBytesW2);
+    const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    // zero the gradient operand buffers (their upper 64 feature columns stay zero: rows
+    // 64..127 of the padded M = 128 weight-gradient GEMMs)
+    for (uint32_t i = t; i < 2 * kBytesG / 16; i += 128) reinterpret_cast<uint4 *>(g2)[i] = make_uint4(0, 0, 0, 0);
+    stage_weights(w, w1s, w2s);
+    if (t < 64) {
+        S.b2[t] = bf16f(w, kOffB2 + t);
+        S.w3[t] = bf16f(w, kOffW3 + t);
+        S.db2[t] = 0.0f;
+        S.dw3[t] = 0.0f;
+    }
+    if (t == 0) {
+        S.db3 = 0.0f;
+        S.loss = 0.0f;
+        tc::mbar_init(&S.mbar, 1);
+    }
+    if (warp == 0) tc::tmem_alloc(&S.tmem, 256);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = S.tmem;
+    const float b3 = bf16f(w, kOffB3);
+    Sync sync{&S.mbar, 0u, true};
+    constexpr uint32_t kD1 = 0, kDW2 = 128, kDW1 = 192;
+    const uint32_t tiles = (P + kTile - 1) / kTile;
+    bool first = true;
+    float my_db3 = 0.0f, my_loss = 0.0f;
+    for (uint32_t tile = blockIdx.x; tile < tiles && sync.ok; tile += gridDim.x) {
+        const uint32_t g = tile * kTile + t;
+        const bool valid = g < P;
+        float4 pt = valid ? pts[g] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        {
+            float f[kF];
+            encode(f3{pt.x, pt.y, pt.z}, f);
+            if (!valid) f[27] = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) store_row8(xs, t, q, kSpX, f + 8 * q);
+        }
+        float z2[kH];
+        const uint64_t mask1 = forward_tile(xs, hs, w1s, w2s, tmem, sync, S.b2, z2);
+        if (!sync.ok) break;
+        // head, loss and its gradient
+        float y = b3;
+#pragma unroll
+        for (int o = 0; o < kH; ++o) y += S.w3[o] * fmaxf(z2[o], 0.0f);
+        const float s = softplus(y);
+        const float e = log1pf(s) - log1pf(fmaxf(pt.w, 0.0f));
+        const float wgt = e < 0.0f ? under_weight : 1.0f;
+        float dy = 0.0f;
+        if (valid) {
+            my_loss += wgt * e * e;
+            dy = 2.0f * wgt * e / (1.0f + s) * sigmoid(y) / (float)P;
+        }
+        my_db3 += dy;
+        float dh2[kH];
+#pragma unroll
+        for (int o = 0; o < kH; ++o) {
+            const float h2 = fmaxf(z2[o], 0.0f);
+            dh2[o] = z2[o] > 0.0f ? dy * S.w3[o] : 0.0f;
+            // warp-reduce this output's dw3 and db2 partials, one shared add per warp
+            float a = dy * h2, b = dh2[o];
+#pragma unroll
+            for (int off = 16; off; off >>= 1) {
+                a += __shfl_xor_sync(kFull, a, off);
+                b += __shfl_xor_sync(kFull, b, off);
+            }
+            if (lane == 0) {
+                atomicAdd(&S.dw3[o], a);
+                atomicAdd(&S.db2[o], b);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) store_row8(g2, t, q, kSpG, dh2 + 8 * q);
+        handoff();
+        if (t == 0) {
+            // dH1 = dH2 W2  (A: dH2 K-major over o;  B: W2 viewed MN-major, N = i, K = o)
+            constexpr uint32_t i_dh1 = tc::idesc_bf16(128, 64, false, true);
+            for (int s4 = 0; s4 < 4; ++s4)
+                tc::mma_bf16(tmem + kD1, tc::smem_desc(tc::smem_addr(g2) + 256 * s4, 128, kSpG),
+                             tc::smem_desc(tc::smem_addr(w2s) + 2 * 1024 * s4, 1024, 128), i_dh1, s4 > 0);
+            // dW2 += dH2^T H1  (A: dH2 MN-major, M = o padded to 128;  B: H1 MN-major, N = i;  K = points)
+            constexpr uint32_t i_dw2 = tc::idesc_bf16(128, 64, true, true);
+            for (int s8 = 0; s8 < 8; ++s8)
+                tc::mma_bf16(tmem + kDW2, tc::smem_desc(tc::smem_addr(g2) + 2 * kSpG * s8, kSpG, 128),
+                             tc::smem_desc(tc::smem_addr(hs) + 2 * kSpH * s8, kSpH, 128), i_dw2, !(first && s8 == 0));
+        }
+        sync.complete();
+        if (!sync.ok) break;
+        {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                float v[16];
+                tc::tmem_ld16(tc::tmem_at(tmem, 32 * warp, kD1 + 16 * j), v);
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    if (!((mask1 >> (16 * j + q)) & 1ull)) v[q] = 0.0f;
+                store_row8(g1, t, 2 * j, kSpG, v);
+                store_row8(g1, t, 2 * j + 1, kSpG, v + 8);
+            }
+        }
+        handoff();
+        if (t == 0) {
+            // dW1 += dH1^T X  (A: dH1 MN-major, M = o padded;  B: X MN-major, N = i = 32;  K = points)
+            constexpr uint32_t i_dw1 = tc::idesc_bf16(128, 32, true, true);
+            for (int s8 = 0; s8 < 8; ++s8)
+                tc::mma_bf16(tmem + kDW1, tc::smem_desc(tc::smem_addr(g1) + 2 * kSpG * s8, kSpG, 128),
+                             tc::smem_desc(tc::smem_addr(xs) + 2 * kSpX * s8, kSpX, 128), i_dw1, !(first && s8 == 0));
+        }
+        sync.complete();
+        first = false;
+    }
+    // flush: per-CTA weight gradients from TMEM (rows o = lanes 0..63: warps 0 and 1)
+    if (sync.ok && !first) {
+        if (warp < 2) {
+            const uint32_t o = t;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                float v[16];
+                tc::tmem_ld16(tc::tmem_at(tmem, 32 * warp, kDW2 + 16 * j), v);
+#pragma unroll
+                for (int q = 0; q < 16; ++q) atomicAdd(&grad[kOffW2 + o * 64 + 16 * j + q], v[q]);
+            }
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                float v[16];
+                tc::tmem_ld16(tc::tmem_at(tmem, 32 * warp, kDW1 + 16 * j), v);
+#pragma unroll
+                for (int q = 0; q < 16; ++q) atomicAdd(&grad[o * 32 + 16 * j + q], v[q]);
+            }
+        }
+        for (int off = 16; off; off >>= 1) {
+            my_db3 += __shfl_xor_sync(kFull, my_db3, off);
+            my_loss += __shfl_xor_sync(kFull, my_loss, off);
+        }
+        if (lane == 0) {
+            atomicAdd(&S.db3, my_db3);
+            atomicAdd(&S.loss, my_loss);
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (sync.ok && !first) {
+        if (t < 64) {
+            atomicAdd(&grad[kOffB2 + t], S.db2[t]);
+            atomicAdd(&grad[kOffW3 + t], S.dw3[t]);
+        }
+        if (t == 0) {
+            atomicAdd(&grad[kOffB3], S.db3);
+            atomicAdd(loss_out, S.loss / (float)P);
+        }
+    }
+    if (warp == 0) tc::tmem_dealloc(tmem, 256);
+}
+
+// ---- inference --------------------------------------------------------------------------
+
+struct InferSmem {
+    float b2[64], w3[64];
+    uint64_t mbar;
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ float infer_point(uint8_t *xs, uint8_t *hs, uint8_t *w1s, uint8_t *w2s, uint32_t tmem,
+                                             Sync &sync, const InferSmem &S, float b3, f3 p, bool valid) {
+    float f[kF];
+    encode(p, f);
+    if (!valid) f[27] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) store_row8(xs, threadIdx.x, q, kSpX, f + 8 * q);
+    float z2[kH];
+    forward_tile(xs, hs, w1s, w2s, tmem, sync, S.b2, z2);
+    float y = b3;
+#pragma unroll
+    for (int o = 0; o < kH; ++o) y += S.w3[o] * fmaxf(z2[o], 0.0f);
+    return softplus(y);
+}
+
+// Density bound at points [P][4] (xyz used), or — when rays is non-null — at the 64 coarse
+// points of every ray: p = o + d t, t = (j + 0.5) L / 64, L = (sdf_count - 1) interval.
+__global__ void __launch_bounds__(128) mlp_infer_kernel(const float4 *__restrict__ pts, uint32_t P,
+                                                        const qsdvr_ray_info *__restrict__ rays,
+                                                        const float *__restrict__ origin,
+                                                        const float *__restrict__ dir, uint32_t nrays,
+                                                        float interval, const __nv_bfloat16 *__restrict__ w,
+                                                        float *__restrict__ out) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *xs = smem;
+    uint8_t *hs = xs + kBytesX;
+    uint8_t *w1s = hs + kBytesH;
+    uint8_t *w2s = w1s + kBytesW1;
+    InferSmem &S = *reinterpret_cast<InferSmem *>(w2s + kBytesW2);
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+    stage_weights(w, w1s, w2s);
+    if (t < 64) {
+        S.b2[t] = bf16f(w, kOffB2 + t);
+        S.w3[t] = bf16f(w, kOffW3 + t);
+    }
+    if (t == 0) tc::mbar_init(&S.mbar, 1);
+    if (warp == 0) tc::tmem_alloc(&S.tmem, 128);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = S.tmem;
+    const float b3 = bf16f(w, kOffB3);
+    Sync sync{&S.mbar, 0u, true};
+    const uint32_t total = rays ? nrays * 64u : P;
+    const uint32_t tiles = (total + kTile - 1) / kTile;
+    for (uint32_t tile = blockIdx.x; tile < tiles && sync.ok; tile += gridDim.x) {
+        const uint32_t g = tile * kTile + t;
+        const bool valid = g < total;
+        f3 p{0.0f, 0.0f, 0.0f};
+        if (valid) {
+            if (rays) {
+                const uint32_t r = g >> 6, j = g & 63;
+                const uint32_t ns = rays[r].sdf_count;
+                const float L = ns > 1 ? (float)(ns - 1) * interval : 0.0f;
+                const float tt = ((float)j + 0.5f) * (L / 64.0f);
+                const f3 o = load3(origin + 3ull * r), d = load3(dir + 3ull * r);
+                p = f3{fmaf(d.x, tt, o.x), fmaf(d.y, tt, o.y), fmaf(d.z, tt, o.z)};
+            } else {
+                const float4 q = pts[g];
+                p = f3{q.x, q.y, q.z};
+            }
+        }
+        const float s = infer_point(xs, hs, w1s, w2s, tmem, sync, S, b3, p, valid);
+        if (valid && sync.ok) out[g] = s;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 128);
+}
+
+// ---- coarse-to-fine sampling ---------------------------------------------------------------
+// One warp per ray: coarse opacity a_j = 1 - exp(-s_j L/64), weights T_j a_j, a pdf mixed with
+// 5% uniform, and the 33 fine SDF positions at the CDF quantiles k/32 (t_0 = 0, t_32 = L).
+__global__ void __launch_bounds__(256) proposal_sample_kernel(const qsdvr_ray_info *__restrict__ rays,
+                                                              uint32_t nrays, float interval,
+                                                              const float *__restrict__ dens,
+                                                              float *__restrict__ tlist) {
+    __shared__ float cdf_s[8][65];
+    const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t r = blockIdx.x * 8 + w;
+    if (r >= nrays) return;
+    const uint32_t ns = rays[r].sdf_count;
+    const float L = ns > 1 ? (float)(ns - 1) * interval : 0.0f;
+    const float delta = L / 64.0f;
+    float *cdf = cdf_s[w];
+    // two coarse bins per lane: j = 2 lane, 2 lane + 1
+    const float s0 = dens[64ull * r + 2 * lane], s1 = dens[64ull * r + 2 * lane + 1];
+    const float t0 = expf(-fmaxf(s0, 0.0f) * delta), t1 = expf(-fmaxf(s1, 0.0f) * delta);  // 1 - alpha
+    float incl = t0 * t1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float v = __shfl_up_sync(kFull, incl, o);
+        if ((int)lane >= o) incl *= v;
+    }
+    float T = __shfl_up_sync(kFull, incl, 1);
+    if (lane == 0) T = 1.0f;
+    const float w0 = T * (1.0f - t0), w1 = T * t0 * (1.0f - t1);
+    float sum = w0 + w1;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+    const float mix = 0.05f / 64.0f;
+    const float p0 = sum > 0.0f ? 0.95f * w0 / sum + mix : 1.0f / 64.0f;
+    const float p1 = sum > 0.0f ? 0.95f * w1 / sum + mix : 1.0f / 64.0f;
+    float c = p0 + p1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float v = __shfl_up_sync(kFull, c, o);
+        if ((int)lane >= o) c += v;
+    }
+    const float total = __shfl_sync(kFull, c, 31);
+    cdf[2 * lane + 1] = (c - p1) / total;
+    cdf[2 * lane + 2] = c / total;
+    if (lane == 0) cdf[0] = 0.0f;
+    __syncwarp();
+    for (uint32_t k = lane; k <= 32; k += 32) {
+        float tk;
+        if (k == 0) {
+            tk = 0.0f;
+        } else if (k == 32) {
+            tk = L;
+        } else {
+            const float q = (float)k / 32.0f;
+            int lo = 0, hi = 64;  // cdf[lo] <= q < cdf[hi]
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (cdf[mid] <= q) lo = mid; else hi = mid;
+            }
+            const float span = cdf[lo + 1] - cdf[lo];
+            const float frac = span > 0.0f ? (q - cdf[lo]) / span : 0.5f;
+            tk = fminf(((float)lo + fminf(fmaxf(frac, 0.0f), 1.0f)) * delta, L);
+        }
+        tlist[33ull * r + k] = tk;
+    }
+}
+
+// ---- training targets from the renderer ------------------------------------------------------
+// One warp per ray: render sample i of ray r (position midpoint(o, d, i, interval), the
+// reference's render sample) with the renderer's alpha gives the target density
+// -log(1 - alpha) / interval.
+__global__ void __launch_bounds__(256) proposal_targets_kernel(const qsdvr_ray_info *__restrict__ rays,
+                                                               const float *__restrict__ origin,
+                                                               const float *__restrict__ dir, uint32_t nrays,
+                                                               float interval, const float *__restrict__ alpha,
+                                                               uint64_t capacity, float4 *__restrict__ pts) {
+    const uint32_t r = (blockIdx.x * 256u + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (r >= nrays) return;
+    const qsdvr_ray_info info = rays[r];
+    if ((uint64_t)info.render_offset + info.render_count > capacity) {
+        if (lane == 0) flag_error(QSDVR_DEVERR_CAPACITY);
+        return;
+    }
+    const f3 o = load3(origin + 3ull * r), d = load3(dir + 3ull * r);
+    for (uint32_t i = lane; i < info.render_count; i += 32) {
+        const uint64_t m = (uint64_t)info.render_offset + i;
+        const f3 p = midpoint(o, d, i, interval);
+        const float a = fminf(fmaxf(alpha[m], 0.0f), 1.0f - 1e-6f);
+        pts[m] = make_float4(p.x, p.y, p.z, -log1pf(-a) / interval);
+    }
+}
+
+constexpr size_t train_smem() { return kBytesX + kBytesH + 2 * kBytesG + kBytesW1 + kBytesW2 + sizeof(TrainSmem); }
+// At most 4 inference CTAs per SM (4 x 128 TMEM columns): request 52 KiB of shared memory,
+// which is more than the kernel uses, so that a fifth never becomes resident and waits in
+// tcgen05.alloc.  Training CTAs (256 columns) are limited to 2 per SM by their real use.
+constexpr size_t infer_smem() {
+    return kBytesX + kBytesH + kBytesW1 + kBytesW2 + sizeof(InferSmem) > 52 * 1024
+               ? kBytesX + kBytesH + kBytesW1 + kBytesW2 + sizeof(InferSmem)
+               : 52 * 1024;
+}
+
+unsigned persistent_blocks(const void *fn, size_t smem, uint32_t tiles) {
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, smem);
+    uint64_t b = (uint64_t)sms * (per_sm > 0 ? per_sm : 1);
+    if (b > tiles) b = tiles;
+    return (unsigned)(b ? b : 1);
+}
+
+}  // namespace
+}  // namespace qsdvr
+
+using namespace qsdvr;
+
+extern "C" int qsdvr_mlp_train(const float *points, uint32_t count, const void *params_bf16, float under_weight,
+                               float *grad, float *loss, cudaStream_t stream) {
+    if (count == 0) return QSDVR_OK;
+    if (!points || !params_bf16 || !grad || !loss)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_mlp_train: null pointer");
+    if (!aligned(points, 16) || !aligned(params_bf16, 16))
+        return set_error(QSDVR_ERR_ALIGNMENT, "qsdvr_mlp_train: points and params need 16-byte alignment");
+    const size_t smem = train_smem();
+    static bool configured = false;
+    if (!configured) {
+        const int st = check_cuda(
+            cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+            "qsdvr_mlp_train: smem attribute");
+        if (st != QSDVR_OK) return st;
+        configured = true;
+    }
+    const uint32_t tiles = (count + kTile - 1) / kTile;
+    const unsigned blocks = persistent_blocks((const void *)mlp_train_kernel, smem, tiles);
+    mlp_train_kernel<<<blocks, 128, smem, stream>>>(reinterpret_cast<const float4 *>(points), count,
+                                                    static_cast<const __nv_bfloat16 *>(params_bf16), under_weight,
+                                                    grad, loss);
+    return check_launch("qsdvr_mlp_train");
+}
+
+extern "C" int qsdvr_mlp_density(const float *points, uint32_t count, const qsdvr_ray_info *rays, const float *origin,
+                                 const float *dir, uint32_t ray_count, float interval, const void *params_bf16,
+                                 float *out, cudaStream_t stream) {
+    const uint32_t total = rays ? ray_count * 64u : count;
+    if (total == 0) return QSDVR_OK;
+    if (!params_bf16 || !out || (rays ? (!origin || !dir) : !points))
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_mlp_density: null pointer");
+    if ((points && !aligned(points, 16)) || !aligned(params_bf16, 16))
+        return set_error(QSDVR_ERR_ALIGNMENT, "qsdvr_mlp_density: points and params need 16-byte alignment");
+    if (rays && ray_count > (1u << 25))
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_mlp_density: too many rays");
+    const size_t smem = infer_smem();
+    static bool configured = false;
+    if (!configured) {
+        const int st = check_cuda(
+            cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+            "qsdvr_mlp_density: smem attribute");
+        if (st != QSDVR_OK) return st;
+        configured = true;
+    }
+    const uint32_t tiles = (total + kTile - 1) / kTile;
+    const unsigned blocks = persistent_blocks((const void *)mlp_infer_kernel, smem, tiles);
+    mlp_infer_kernel<<<blocks, 128, smem, stream>>>(reinterpret_cast<const float4 *>(points), count, rays, origin, dir,
+                                                    ray_count, interval,
+                                                    static_cast<const __nv_bfloat16 *>(params_bf16), out);
+    return check_launch("qsdvr_mlp_density");
+}
+
+extern "C" int qsdvr_proposal_sample(const qsdvr_ray_info *rays, uint32_t ray_count, float interval,
+                                     const float *coarse_density, float *tlist, cudaStream_t stream) {
+    if (ray_count == 0) return QSDVR_OK;
+    if (!rays || !coarse_density || !tlist)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_proposal_sample: null pointer");
+    proposal_sample_kernel<<<grid_for(ray_count, 8), 256, 0, stream>>>(rays, ray_count, interval, coarse_density, tlist);
+    return check_launch("qsdvr_proposal_sample");
+}
+
+extern "C" int qsdvr_proposal_targets(const qsdvr_ray_info *rays, const float *origin, const float *dir,
+                                      uint32_t ray_count, float interval, const float *alpha, uint64_t sample_count,
+                                      float *points, cudaStream_t stream) {
+    if (ray_count == 0) return QSDVR_OK;
+    if (!rays || !origin || !dir || !alpha || !points)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_proposal_targets: null pointer");
+    if (!aligned(points, 16)) return set_error(QSDVR_ERR_ALIGNMENT, "qsdvr_proposal_targets: points alignment");
+    proposal_targets_kernel<<<grid_for((uint64_t)ray_count * 32, 256), 256, 0, stream>>>(
+        rays, origin, dir, ray_count, interval, alpha, sample_count, reinterpret_cast<float4 *>(points));
+    return check_launch("qsdvr_proposal_targets");
+}

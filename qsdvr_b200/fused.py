@@ -30,7 +30,8 @@ class RenderArgs(ctypes.Structure):
     _fields_ = [("rays", P), ("origin", P), ("dir", P), ("ray_count", U32), ("reso", U32), ("interval", F32),
                 ("logistic_coef", F32), ("mode", I32), ("storage", I32), ("transmittance", I32), ("sh_degree", I32),
                 ("sdf_grid", P), ("data", P), ("color", P), ("target", P), ("grad_color", P), ("sdf_grad", P),
-                ("data_grad", P), ("loss", P), ("grad_scale", F32), ("workspace", P), ("workspace_bytes", ctypes.c_uint64)]
+                ("data_grad", P), ("loss", P), ("grad_scale", F32), ("workspace", P), ("workspace_bytes", ctypes.c_uint64),
+                ("tlist", P), ("sample_alpha", P), ("sample_capacity", ctypes.c_uint64)]
 
 
 _lib.extra_signatures({
@@ -93,7 +94,7 @@ def _grid_storage(sdf_grid, data, R):
 
 def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat", transmittance="product",
               color=None, target=None, grad_color=None, sdf_grad=None, data_grad=None, loss=None,
-              grad_scale=0.0, persistent=True) -> RenderArgs:
+              grad_scale=0.0, persistent=True, tlist=None, sample_alpha=None) -> RenderArgs:
     dev, n = _check_batch(rays, origin, direction)
     a = RenderArgs()
     a.rays, a.origin, a.dir = _ptr(rays), _ptr(origin), _ptr(direction)
@@ -108,6 +109,14 @@ def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="
     a.sdf_grad, a.data_grad, a.loss = _ptr(sdf_grad), _ptr(data_grad), _ptr(loss)
     a.grad_scale = float(grad_scale)
     a.workspace, a.workspace_bytes = None, 0
+    if tlist is not None:
+        if tlist.device != dev or tlist.dtype != torch.float32 or tlist.shape != (n, 33) or not tlist.is_contiguous():
+            raise ValueError(f"tlist must be a contiguous float32 [N,33] tensor on {dev}")
+        a.tlist = tlist.data_ptr()
+    if sample_alpha is not None:
+        if sample_alpha.device != dev or sample_alpha.dtype != torch.float32 or not sample_alpha.is_contiguous():
+            raise ValueError(f"sample_alpha must be a contiguous float32 tensor on {dev}")
+        a.sample_alpha, a.sample_capacity = _ptr(sample_alpha), sample_alpha.numel()
     if persistent and n:
         with torch.cuda.device(dev):
             ws = workspace(dev, a)
@@ -120,20 +129,22 @@ def _stream(dev):
 
 
 def render_forward(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat",
-                   transmittance="product", color=None, persistent=True):
-    """Colour of every ray [N,3]."""
+                   transmittance="product", color=None, persistent=True, tlist=None, sample_alpha=None):
+    """Colour of every ray [N,3].  ``tlist`` [N,33]: render at those SDF positions (32 render
+    samples per ray at their midpoints) instead of the uniform march; ``sample_alpha``: also
+    write every render sample's alpha at the ray's render offset."""
     dev, n = _check_batch(rays, origin, direction)
     if color is None:
         color = torch.empty((n, 3), dtype=torch.float32, device=dev)
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color,
-                  persistent=persistent)
+                  persistent=persistent, tlist=tlist, sample_alpha=sample_alpha)
     with torch.cuda.device(dev):
         call("qsdvr_render_forward", ctypes.byref(a), _stream(dev))
     return color
 
 
 def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
-                    mode="compat", transmittance="product", persistent=True):
+                    mode="compat", transmittance="product", persistent=True, tlist=None):
     """Accumulate dL/d(sdf_grid) and dL/d(data) (fp32) for a given dL/dcolor."""
     dev, n = _check_batch(rays, origin, direction)
     for t, nm, shape in ((sdf_grad, "sdf_grad", sdf_grid.numel()), (data_grad, "data_grad", data.numel())):
@@ -141,13 +152,14 @@ def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, i
             raise ValueError(f"{nm} must be a contiguous float32 tensor shaped like its grid")
     g = grad_color.contiguous().float()
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, grad_color=g,
-                  sdf_grad=sdf_grad, data_grad=data_grad, persistent=persistent)
+                  sdf_grad=sdf_grad, data_grad=data_grad, persistent=persistent, tlist=tlist)
     with torch.cuda.device(dev):
         call("qsdvr_render_backward", ctypes.byref(a), _stream(dev))
 
 
 def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
-                 mode="compat", transmittance="product", loss=None, color=None, persistent=True):
+                 mode="compat", transmittance="product", loss=None, color=None, persistent=True, tlist=None,
+                 sample_alpha=None):
     """Forward + MSE (mean over N x 3) + backward in one launch.  Returns (color, loss_sum)
     where loss_sum accumulates sum |color - target|^2 (divide by 3N for the mean)."""
     dev, n = _check_batch(rays, origin, direction)
@@ -157,7 +169,8 @@ def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval
         loss = torch.zeros(1, dtype=torch.float32, device=dev)
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color,
                   target=target.contiguous(), sdf_grad=sdf_grad, data_grad=data_grad, loss=loss,
-                  grad_scale=2.0 / (3.0 * max(n, 1)), persistent=persistent)
+                  grad_scale=2.0 / (3.0 * max(n, 1)), persistent=persistent, tlist=tlist,
+                  sample_alpha=sample_alpha)
     with torch.cuda.device(dev):
         call("qsdvr_render_train", ctypes.byref(a), _stream(dev))
     return color, loss
@@ -201,7 +214,8 @@ class DenseRenderGrid(nn.Module):
     refreshed by ``sync_storage()`` (call it after each optimizer step)."""
 
     def __init__(self, reso: int = 128, logisticCoef: float = 5.0, interval: float = 4.0 / 256, mode: str = "compat",
-                 storage: str = "f32", transmittance: str | None = None, device="cuda", sdf_grid=None, data=None):
+                 storage: str = "f32", transmittance: str | None = None, device="cuda", sdf_grid=None, data=None,
+                 sh_degree: int = 2):
         super().__init__()
         self.reso, self.interval, self.mode, self.storage = reso, interval, mode, storage
         self.logisticCoef = logisticCoef
@@ -211,14 +225,17 @@ class DenseRenderGrid(nn.Module):
 
             sdf_grid = sphere_grid(reso, 0.5, 0.0, device=device)
         if data is None:
-            data = torch.zeros(((reso + 1) ** 3, 32), dtype=torch.float32, device=device)
-            data[:, 31] = 1
-            data[:, 30] = 0.1
-            data[:, 27:30] = 1
+            # models/render.py:215-223 (ao 1, metallic 0.1, diffuse 1, SH DC 0.5); degree 3
+            # keeps the same values after its 48 SH channels
+            nsh = 3 * (sh_degree + 1) ** 2
+            data = torch.zeros(((reso + 1) ** 3, 32 if sh_degree == 2 else 64), dtype=torch.float32, device=device)
+            data[:, nsh + 4] = 1
+            data[:, nsh + 3] = 0.1
+            data[:, nsh:nsh + 3] = 1
             data[:, 0:3] = 0.5
         g = sdf_grid.reshape(-1, sdf_grid.shape[-1])
         self.sdfGrid = nn.Parameter(pad_grid7(g) if g.shape[1] == 7 else g.contiguous().clone())
-        self.renderData = nn.Parameter(data.reshape(-1, 32).contiguous().clone())
+        self.renderData = nn.Parameter(data.reshape((reso + 1) ** 3, -1).contiguous().clone())
         self._copies = None
         self.sync_storage()
 

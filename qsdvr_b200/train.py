@@ -2,12 +2,17 @@
 random ray batches, forward + MSE + backward, Adam), reporting loss, PSNR on held-out
 rays, step time and peak device memory.
 
-    python -m qsdvr_b200.train --reso 256 --steps 1000 --rays 65536 --lr 1e-2
+    python -m qsdvr_b200.train --reso 256 --steps 1000 --rays 65536 --lr 1e-2 [--proposal]
 
 Targets come from a seeded procedural ground-truth scene rendered once for every pixel of
 every view; the model starts from a sphere SDF and constant appearance (models/render.py:
 215-223).  Per-sample values are recomputed in the backward, so memory beyond the grids,
 their gradients and Adam state is O(rays).
+
+``--proposal`` trains the grid at the proposal network's 32 fine samples per ray (64 coarse
+MLP evaluations place them) instead of the uniform march.  The network is trained online
+every step on the per-sample alphas of a uniform-march forward over part of the batch.
+Held-out PSNR is always measured with the uniform march (the judge).
 """
 from __future__ import annotations
 
@@ -23,9 +28,9 @@ from .camera import Camera
 from .optim import FusedGridAdam
 
 
-def build(reso, views, size, focal, radius, interval, k, seed, device):
+def build(reso, views, size, focal, radius, interval, k, seed, device, sh_degree=2):
     gt_sdf = fused.pad_grid7(scenes.procedural_grid(reso, seed=seed, device=device).reshape(-1, 7))
-    gt_data = scenes.appearance(reso, seed=seed, device=device, procedural=True)
+    gt_data = scenes.appearance(reso, seed=seed, device=device, procedural=True, sh_degree=sh_degree)
     cams = scenes.hemisphere_cameras(views, radius, size, size, focal, 2.0, 6.0, seed=seed)
     rays, origin, direction, target = [], [], [], []
     mask = torch.ones(size * size, dtype=torch.bool)
@@ -45,7 +50,7 @@ def psnr(mse: float) -> float:
     return -10.0 * math.log10(max(mse, 1e-12))
 
 
-def main(argv=None):
+def parser():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reso", type=int, default=256)
     ap.add_argument("--steps", type=int, default=1000)
@@ -57,59 +62,106 @@ def main(argv=None):
     ap.add_argument("--k", type=float, default=5.0)
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16"])
     ap.add_argument("--mode", default="fixed", choices=["fixed", "compat"])
+    ap.add_argument("--sh", type=int, default=2, choices=[2, 3])
+    ap.add_argument("--proposal", action="store_true", help="train at the proposal network's fine samples")
+    ap.add_argument("--proposal-rays", type=int, default=4096, help="rays of the per-step uniform pass")
+    ap.add_argument("--proposal-points", type=int, default=65536, help="MLP training points per step")
+    ap.add_argument("--proposal-lr", type=float, default=5e-3)
     ap.add_argument("--log-every", type=int, default=100)
     ap.add_argument("--seed", type=int, default=0)
-    a = ap.parse_args(argv)
+    return ap
+
+
+def run(a, data=None, quiet=False):
+    """Train per ``a`` (parser() namespace).  ``data``: (rays, origin, dir, target) to reuse
+    a built scene.  Returns the summary dict; its "render_ms" is the device time of the
+    render part of the steps (forward + backward, and for --proposal the coarse MLP, the
+    sampler and the online network update), "optimizer_ms" that of the grid Adam steps."""
+    from .proposal import ProposalNet
+
     dev = torch.device("cuda", torch.cuda.current_device())
     R = a.reso
-    rays, origin, direction, target = build(R, a.views, a.size, 1111.1 * a.size / 800, 4.03, a.interval, a.k, a.seed,
-                                            dev)
+    if data is None:
+        data = build(R, a.views, a.size, 1111.1 * a.size / 800, 4.03, a.interval, a.k, a.seed, dev, a.sh)
+    rays, origin, direction, target = data
     total = rays.shape[0]
     gen = torch.Generator(device=dev).manual_seed(a.seed + 1)
     held = torch.randint(0, total, (a.rays,), generator=gen, device=dev)
     torch.cuda.reset_peak_memory_stats(dev)
     base_mem = torch.cuda.memory_allocated(dev)
-    model = fused.DenseRenderGrid(R, a.k, a.interval, mode=a.mode, storage=a.storage, device=dev)
+    model = fused.DenseRenderGrid(R, a.k, a.interval, mode=a.mode, storage=a.storage, device=dev, sh_degree=a.sh)
     copies = dict(zip((model.sdfGrid, model.renderData), model._copies)) if a.storage == "bf16" else None
     opt = FusedGridAdam(model.parameters(), lr=a.lr, bf16_copies=copies)
     model.sdfGrid.grad = torch.zeros_like(model.sdfGrid)
     model.renderData.grad = torch.zeros_like(model.renderData)
+    net = ProposalNet(dev, seed=a.seed, lr=a.proposal_lr) if a.proposal else None
+    pgen = torch.Generator(device=dev).manual_seed(a.seed + 2)
     loss = torch.zeros(1, dtype=torch.float32, device=dev)
     log = []
 
     def evaluate():
         sg, dg = model.grids()
-        col = fused.render_forward(rays[held], origin[held], direction[held], sg.detach(), dg.detach(), R, a.interval,
-                                   a.k, a.mode, model.transmittance)
-        return float(((col - target[held]) ** 2).mean())
+        args = (rays[held], origin[held], direction[held], sg.detach(), dg.detach(), R, a.interval, a.k, a.mode,
+                model.transmittance)
+        col = fused.render_forward(*args)
+        out = {"uniform": float(((col - target[held]) ** 2).mean())}
+        if net is not None:
+            colp = net.render(*args)
+            out["proposal"] = float(((colp - target[held]) ** 2).mean())
+        return out
 
-    start_mse = evaluate()
+    start = evaluate()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for step in range(1, a.steps + 1):
         idx = torch.randint(0, total, (a.rays,), generator=gen, device=dev)
+        r, o, d, tg = rays[idx], origin[idx], direction[idx], target[idx]
         sg, dg = model.grids()
+        sg, dg = sg.detach(), dg.detach()
+        e0, e1, e2 = ev[step - 1]
+        e0.record()
         loss.zero_()
-        fused.render_train(target[idx], rays[idx], origin[idx], direction[idx], sg.detach(), dg.detach(), R,
-                           a.interval, a.k, model.sdfGrid.grad, model.renderData.grad, a.mode, model.transmittance,
-                           loss=loss)
+        tlist = None
+        if net is not None:
+            n = min(a.proposal_rays, a.rays)
+            net.online_step(r[:n], o[:n], d[:n], sg, dg, R, a.interval, a.k, a.mode, model.transmittance,
+                            points=a.proposal_points, generator=pgen)
+            tlist = net.sample(r, o, d, a.interval)
+        fused.render_train(tg, r, o, d, sg, dg, R, a.interval, a.k, model.sdfGrid.grad, model.renderData.grad,
+                           a.mode, model.transmittance, loss=loss, tlist=tlist)
+        e1.record()
         opt.step()  # Adam on the fp32 masters; zeroes the gradients, refreshes bf16 copies
-        if step % a.log_every == 0 or step == a.steps:
+        e2.record()
+        if not quiet and (step % a.log_every == 0 or step == a.steps):
             torch.cuda.synchronize()
             mse = float(loss) / (3 * a.rays)
             log.append({"step": step, "train_mse": mse, "elapsed_s": round(time.perf_counter() - t0, 3)})
             print(json.dumps(log[-1]), flush=True)
     torch.cuda.synchronize()
     elapsed = time.perf_counter() - t0
-    end_mse = evaluate()
+    render_ms = sum(e0.elapsed_time(e1) for e0, e1, _ in ev)
+    opt_ms = sum(e1.elapsed_time(e2) for _, e1, e2 in ev)
+    end = evaluate()
     out = {"reso": R, "steps": a.steps, "rays_per_step": a.rays, "lr": a.lr, "storage": a.storage, "mode": a.mode,
+           "sh_degree": a.sh, "k": a.k, "method": "proposal 64 coarse + 32 fine" if net else "uniform march",
            "ms_per_step": round(1e3 * elapsed / a.steps, 3), "train_rays_per_s": round(a.steps * a.rays / elapsed),
-           "heldout_psnr_start": round(psnr(start_mse), 3), "heldout_psnr_end": round(psnr(end_mse), 3),
+           "render_ms": round(render_ms, 3), "optimizer_ms": round(opt_ms, 3),
+           "render_rays_per_s": round(a.steps * a.rays / (render_ms / 1e3)),
+           "heldout_psnr_start": round(psnr(start["uniform"]), 3), "heldout_psnr_end": round(psnr(end["uniform"]), 3),
            "peak_memory_gb": round(torch.cuda.max_memory_allocated(dev) / 1e9, 3),
            "model_and_state_gb": round((torch.cuda.max_memory_allocated(dev) - base_mem) / 1e9, 3),
            "ray_pool_gb": round(base_mem / 1e9, 3)}
-    print(json.dumps(out), flush=True)
+    if net is not None:
+        out["heldout_psnr_end_proposal_render"] = round(psnr(end["proposal"]), 3)
+    if not quiet:
+        print(json.dumps(out), flush=True)
     return out
+
+
+def main(argv=None):
+    return run(parser().parse_args(argv))
 
 
 if __name__ == "__main__":
