@@ -302,20 +302,33 @@ int qsdvr_mlp_density(const float *points, uint32_t count, const qsdvr_ray_info 
 
 /* One training pass over points [count][4] (x, y, z, target density): accumulates the
  * gradient of mean_p w (log1p(bound) - log1p(target))^2 (w = under_weight where the bound is
- * below the target) into grad [QSDVR_MLP_PARAMS] fp32 and the loss into *loss. */
+ * below the target; points with a negative target contribute nothing) into
+ * grad [QSDVR_MLP_PARAMS] fp32 and the loss into *loss. */
 int qsdvr_mlp_train(const float *points, uint32_t count, const void *params_bf16, float under_weight, float *grad,
                     float *loss, cudaStream_t stream);
 
+/* Launch shape of the persistent MLP kernels for count points (kernel 0: inference,
+ * 1: training): grid size and resident CTAs per SM. */
+int qsdvr_mlp_launch_shape(int kernel, uint32_t count, uint32_t *blocks, int *blocks_per_sm);
+
 /* Fine sample positions [ray_count][33] from the coarse densities [ray_count][64]: inverse
- * CDF of the coarse compositing weights (mixed with 5% uniform) at quantiles k/32. */
-int qsdvr_proposal_sample(const qsdvr_ray_info *rays, uint32_t ray_count, float interval, const float *coarse_density,
-                          float *tlist, cudaStream_t stream);
+ * CDF of the coarse compositing weights, mixed with the fraction uniform_mix (0, 1] of a
+ * uniform density, at quantiles k/32. */
+int qsdvr_proposal_sample(const qsdvr_ray_info *rays, uint32_t ray_count, float interval, float uniform_mix,
+                          const float *coarse_density, float *tlist, cudaStream_t stream);
 
 /* Training points for the proposal network from a uniform-march forward: render sample i
  * of ray r at rays[r].render_offset + i gets (position, -log(1 - alpha) / interval). */
 int qsdvr_proposal_targets(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
                            float interval, const float *alpha, uint64_t sample_count, float *points,
                            cudaStream_t stream);
+
+/* count training points [count][4] drawn at random (counter-based hash of seed and point
+ * index) from the same alphas: a ray uniformly, then one of its render samples uniformly;
+ * a point that finds no ray with samples in 16 draws gets target -1 (ignored in training). */
+int qsdvr_proposal_draw(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
+                        float interval, const float *alpha, uint64_t sample_count, uint32_t count, uint32_t seed,
+                        float *points, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

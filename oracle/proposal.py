@@ -10,9 +10,10 @@ specification the CUDA kernels (qsdvr_b200/csrc/proposal.cu) are checked against
   before the tensor-core GEMMs, and in training the two back-propagated hidden gradients as
   well; the oracle applies the same roundings (round to nearest even) and does every other
   operation in float64.
-* Loss per point: w (log1p(s) - log1p(t))^2, w = under_weight where s < t, mean over points.
+* Loss per point: w (log1p(s) - log1p(t))^2, w = under_weight where s < t, mean over points;
+  points with a negative target are ignored (they still count in the mean's denominator).
 * Sampler: coarse opacity 1 - exp(-s L/64) in 64 equal bins of the in-box segment,
-  compositing weights mixed with 5% uniform, fine SDF positions at the CDF quantiles k/32.
+  compositing weights mixed with a uniform share, fine SDF positions at the CDF quantiles k/32.
 * Targets: density -log(1 - alpha) / interval at each render sample of a uniform march.
 
 Gradients of the MLP restatement are checked against torch autograd of its own forward in
@@ -85,9 +86,10 @@ def train_gradients(params, points, under_weight: float, round_grads: bool = Tru
     P = pts.shape[0]
     f = forward(params, pts)
     w = f["w"]
+    use = pts[:, 3] >= 0.0  # a negative target marks a point to ignore
     t = np.maximum(pts[:, 3].astype(np.float64), 0.0)
     e = np.log1p(f["s"]) - np.log1p(t)
-    wgt = np.where(e < 0.0, under_weight, 1.0)
+    wgt = np.where(use, np.where(e < 0.0, under_weight, 1.0), 0.0)
     loss = float((wgt * e * e).sum() / P)
     dy = 2.0 * wgt * e / (1.0 + f["s"]) / (1.0 + np.exp(-f["y"])) / P
     g = np.zeros(N_PARAMS, np.float64)
@@ -121,7 +123,7 @@ def loss_torch(params: torch.Tensor, points: torch.Tensor, under_weight: float) 
     s = forward_torch(params, points)
     t = torch.clamp(points[:, 3].double(), min=0.0)
     e = torch.log1p(s) - torch.log1p(t)
-    wgt = torch.where(e < 0.0, torch.full_like(e, under_weight), torch.ones_like(e))
+    wgt = torch.where(e < 0.0, torch.full_like(e, under_weight), torch.ones_like(e)) * (points[:, 3] >= 0.0).double()
     return (wgt * e * e).mean()
 
 
@@ -137,7 +139,7 @@ def coarse_points(rays, origin, direction, interval) -> np.ndarray:
     return p.reshape(-1, 3)
 
 
-def sample(rays, interval, coarse_density) -> np.ndarray:
+def sample(rays, interval, coarse_density, uniform_mix: float = 0.05) -> np.ndarray:
     """[N,33] fine SDF positions from [N,64] coarse densities (float64 restatement)."""
     ns = np.asarray(rays)[:, 0].astype(np.int64)
     L = np.where(ns > 1, (ns - 1).astype(np.float32) * np.float32(interval), np.float32(0.0)).astype(np.float64)
@@ -147,7 +149,8 @@ def sample(rays, interval, coarse_density) -> np.ndarray:
     T = np.cumprod(np.concatenate([np.ones((dens.shape[0], 1)), keep[:, :-1]], 1), 1)
     wts = T * (1.0 - keep)
     tot = wts.sum(1, keepdims=True)
-    pdf = np.where(tot > 0.0, 0.95 * wts / np.where(tot > 0.0, tot, 1.0) + 0.05 / 64.0, 1.0 / 64.0)
+    pdf = np.where(tot > 0.0, (1.0 - uniform_mix) * wts / np.where(tot > 0.0, tot, 1.0) + uniform_mix / 64.0,
+                   1.0 / 64.0)
     cdf = np.concatenate([np.zeros((dens.shape[0], 1)), np.cumsum(pdf, 1)], 1)
     cdf /= cdf[:, -1:]
     out = np.zeros((dens.shape[0], 33))

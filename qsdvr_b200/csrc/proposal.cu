@@ -30,6 +30,8 @@ constexpr int kTile = 128;
 constexpr int kF = 32, kH = 64;
 constexpr int kOffW2 = 2048, kOffB2 = 6144, kOffW3 = 6208, kOffB3 = 6272;
 constexpr uint32_t kSpins = 1u << 26;  // bounded mbarrier waits (~ seconds), then give up
+constexpr uint32_t kInferCols = 64;    // TMEM columns of an inference CTA (both layers)
+constexpr uint32_t kTrainCols = 256;   // of a training CTA: forward 0..63, dW2 128..191, dW1 192..223
 
 // shared-memory operand layouts (bytes): element (row, feature) of an activation buffer with
 // point-group stride SP sits at (row/8)*SP + (f/8)*128 + (row%8)*16 + (f%8)*2
@@ -119,45 +121,42 @@ __device__ __forceinline__ void handoff() {
     tc::fence_after_sync();
 }
 
-// Forward of one tile: X (staged) -> H1 (staged, returns relu mask) -> z2 = W2 h1 + b2 (row in registers).
-__device__ __forceinline__ uint64_t forward_tile(uint8_t *xs, uint8_t *hs, uint8_t *w1s, uint8_t *w2s, uint32_t tmem,
+// Forward of one tile: X (staged) -> H1 (staged, returns the relu mask) -> z2 = W2 h1 + b2
+// (this thread's row, in registers).  Both layers accumulate in the same 64 TMEM columns at
+// d1: every thread has read layer 1's result before the barrier that precedes layer 2.
+__device__ __forceinline__ uint64_t forward_tile(uint8_t *xs, uint8_t *hs, uint8_t *w1s, uint8_t *w2s, uint32_t d1,
                                                  Sync &sync, const float *b2, float *z2) {
     const uint32_t t = threadIdx.x, warp = t >> 5;
     constexpr uint32_t i1 = tc::idesc_bf16(128, 64, false, false);
     handoff();
     if (t == 0) {
         for (int s = 0; s < 2; ++s)
-            tc::mma_bf16(tmem + 0, tc::smem_desc(tc::smem_addr(xs) + 256 * s, 128, kSpX),
+            tc::mma_bf16(d1, tc::smem_desc(tc::smem_addr(xs) + 256 * s, 128, kSpX),
                          tc::smem_desc(tc::smem_addr(w1s) + 256 * s, 128, 512), i1, s > 0);
     }
     sync.complete();
     uint64_t mask = 0;
+    {
+        float v[64];
+        tc::tmem_ld64(tc::tmem_at(d1, 32 * warp, 0), v);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        float v[16];
-        tc::tmem_ld16(tc::tmem_at(tmem, 32 * warp, 16 * j), v);
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            if (v[q] > 0.0f) mask |= 1ull << (16 * j + q);
+        for (int q = 0; q < 64; ++q) {
+            if (v[q] > 0.0f) mask |= 1ull << q;
             v[q] = fmaxf(v[q], 0.0f);
         }
-        store_row8(hs, t, 2 * j, kSpH, v);
-        store_row8(hs, t, 2 * j + 1, kSpH, v + 8);
+#pragma unroll
+        for (int g = 0; g < 8; ++g) store_row8(hs, t, g, kSpH, v + 8 * g);
     }
     handoff();
     if (t == 0) {
         for (int s = 0; s < 4; ++s)
-            tc::mma_bf16(tmem + 64, tc::smem_desc(tc::smem_addr(hs) + 256 * s, 128, kSpH),
+            tc::mma_bf16(d1, tc::smem_desc(tc::smem_addr(hs) + 256 * s, 128, kSpH),
                          tc::smem_desc(tc::smem_addr(w2s) + 256 * s, 128, 1024), i1, s > 0);
     }
     sync.complete();
+    tc::tmem_ld64(tc::tmem_at(d1, 32 * warp, 0), z2);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        float v[16];
-        tc::tmem_ld16(tc::tmem_at(tmem, 32 * warp, 64 + 16 * j), v);
-#pragma unroll
-        for (int q = 0; q < 16; ++q) z2[16 * j + q] = v[q] + b2[16 * j + q];
-    }
+    for (int q = 0; q < 64; ++q) z2[q] += b2[q];
     return mask;
 }
 
@@ -170,7 +169,8 @@ struct TrainSmem {
 };
 
 // points [P][4] = (x, y, z, target density).  Loss per point (mean over P):
-// w (log1p(s) - log1p(t))^2 with s = softplus(y) the bound and w = under_weight when s < t.
+// w (log1p(s) - log1p(t))^2 with s = softplus(y) the bound and w = under_weight when s < t;
+// a point with a negative target is ignored (no loss, no gradient; it still counts in P).
 __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict__ pts, uint32_t P,
                                                         const __nv_bfloat16 *__restrict__ w, float under_weight,
                                                         float *__restrict__ grad, float *__restrict__ loss_out) {
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
         S.loss = 0.0f;
         tc::mbar_init(&S.mbar, 1);
     }
-    if (warp == 0) tc::tmem_alloc(&S.tmem, 256);
+    if (warp == 0) tc::tmem_alloc(&S.tmem, kTrainCols);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -211,8 +211,8 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
     float my_db3 = 0.0f, my_loss = 0.0f;
     for (uint32_t tile = blockIdx.x; tile < tiles && sync.ok; tile += gridDim.x) {
         const uint32_t g = tile * kTile + t;
-        const bool valid = g < P;
-        float4 pt = valid ? pts[g] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float4 pt = g < P ? pts[g] : make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        const bool valid = pt.w >= 0.0f;
         {
             float f[kF];
             encode(f3{pt.x, pt.y, pt.z}, f);
@@ -221,14 +221,14 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
             for (int q = 0; q < 4; ++q) store_row8(xs, t, q, kSpX, f + 8 * q);
         }
         float z2[kH];
-        const uint64_t mask1 = forward_tile(xs, hs, w1s, w2s, tmem, sync, S.b2, z2);
+        const uint64_t mask1 = forward_tile(xs, hs, w1s, w2s, tmem + kD1, sync, S.b2, z2);
         if (!sync.ok) break;
         // head, loss and its gradient
         float y = b3;
 #pragma unroll
         for (int o = 0; o < kH; ++o) y += S.w3[o] * fmaxf(z2[o], 0.0f);
         const float s = softplus(y);
-        const float e = log1pf(s) - log1pf(fmaxf(pt.w, 0.0f));
+        const float e = log1pf(s) - log1pf(pt.w);
         const float wgt = e < 0.0f ? under_weight : 1.0f;
         float dy = 0.0f;
         if (valid) {
@@ -271,16 +271,13 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
         sync.complete();
         if (!sync.ok) break;
         {
+            float v[64];
+            tc::tmem_ld64(tc::tmem_at(tmem, 32 * warp, kD1), v);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                float v[16];
-                tc::tmem_ld16(tc::tmem_at(tmem, 32 * warp, kD1 + 16 * j), v);
+            for (int q = 0; q < 64; ++q)
+                if (!((mask1 >> q) & 1ull)) v[q] = 0.0f;
 #pragma unroll
-                for (int q = 0; q < 16; ++q)
-                    if (!((mask1 >> (16 * j + q)) & 1ull)) v[q] = 0.0f;
-                store_row8(g1, t, 2 * j, kSpG, v);
-                store_row8(g1, t, 2 * j + 1, kSpG, v + 8);
-            }
+            for (int gq = 0; gq < 8; ++gq) store_row8(g1, t, gq, kSpG, v + 8 * gq);
         }
         handoff();
         if (t == 0) {
@@ -333,7 +330,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
             atomicAdd(loss_out, S.loss / (float)P);
         }
     }
-    if (warp == 0) tc::tmem_dealloc(tmem, 256);
+    if (warp == 0) tc::tmem_dealloc(tmem, kTrainCols);
 }
 
 // ---- inference --------------------------------------------------------------------------
@@ -344,24 +341,27 @@ struct InferSmem {
     uint32_t tmem;
 };
 
-__device__ __forceinline__ float infer_point(uint8_t *xs, uint8_t *hs, uint8_t *w1s, uint8_t *w2s, uint32_t tmem,
-                                             Sync &sync, const InferSmem &S, float b3, f3 p, bool valid) {
-    float f[kF];
-    encode(p, f);
-    if (!valid) f[27] = 0.0f;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) store_row8(xs, threadIdx.x, q, kSpX, f + 8 * q);
-    float z2[kH];
-    forward_tile(xs, hs, w1s, w2s, tmem, sync, S.b2, z2);
-    float y = b3;
-#pragma unroll
-    for (int o = 0; o < kH; ++o) y += S.w3[o] * fmaxf(z2[o], 0.0f);
-    return softplus(y);
+// Point g of the inference input: points[g].xyz, or coarse point g % 64 of ray g / 64 at
+// t = (j + 0.5) L / 64, L = (sdf_count - 1) interval.
+__device__ __forceinline__ f3 infer_input(const float4 *__restrict__ pts, const qsdvr_ray_info *__restrict__ rays,
+                                          const float *__restrict__ origin, const float *__restrict__ dir,
+                                          float interval, uint32_t g) {
+    if (rays) {
+        const uint32_t r = g >> 6, j = g & 63;
+        const uint32_t ns = rays[r].sdf_count;
+        const float L = ns > 1 ? (float)(ns - 1) * interval : 0.0f;
+        const float tt = ((float)j + 0.5f) * (L / 64.0f);
+        const f3 o = load3(origin + 3ull * r), d = load3(dir + 3ull * r);
+        return f3{fmaf(d.x, tt, o.x), fmaf(d.y, tt, o.y), fmaf(d.z, tt, o.z)};
+    }
+    const float4 q = pts[g];
+    return f3{q.x, q.y, q.z};
 }
 
 // Density bound at points [P][4] (xyz used), or — when rays is non-null — at the 64 coarse
-// points of every ray: p = o + d t, t = (j + 0.5) L / 64, L = (sdf_count - 1) interval.
-__global__ void __launch_bounds__(128) mlp_infer_kernel(const float4 *__restrict__ pts, uint32_t P,
+// points of every ray.  Persistent: each CTA walks tiles of 128 points and fetches the next
+// tile's input before waiting on this tile's MMAs.
+__global__ void __launch_bounds__(128, 5) mlp_infer_kernel(const float4 *__restrict__ pts, uint32_t P,
                                                         const qsdvr_ray_info *__restrict__ rays,
                                                         const float *__restrict__ origin,
                                                         const float *__restrict__ dir, uint32_t nrays,
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float4 *__restrict
         S.w3[t] = bf16f(w, kOffW3 + t);
     }
     if (t == 0) tc::mbar_init(&S.mbar, 1);
-    if (warp == 0) tc::tmem_alloc(&S.tmem, 128);
+    if (warp == 0) tc::tmem_alloc(&S.tmem, kInferCols);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -389,36 +389,41 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float4 *__restrict
     Sync sync{&S.mbar, 0u, true};
     const uint32_t total = rays ? nrays * 64u : P;
     const uint32_t tiles = (total + kTile - 1) / kTile;
-    for (uint32_t tile = blockIdx.x; tile < tiles && sync.ok; tile += gridDim.x) {
-        const uint32_t g = tile * kTile + t;
+    uint32_t tile = blockIdx.x;
+    uint32_t g = tile * kTile + t;
+    f3 p = g < total ? infer_input(pts, rays, origin, dir, interval, g) : f3{0.0f, 0.0f, 0.0f};
+    while (tile < tiles && sync.ok) {
         const bool valid = g < total;
-        f3 p{0.0f, 0.0f, 0.0f};
-        if (valid) {
-            if (rays) {
-                const uint32_t r = g >> 6, j = g & 63;
-                const uint32_t ns = rays[r].sdf_count;
-                const float L = ns > 1 ? (float)(ns - 1) * interval : 0.0f;
-                const float tt = ((float)j + 0.5f) * (L / 64.0f);
-                const f3 o = load3(origin + 3ull * r), d = load3(dir + 3ull * r);
-                p = f3{fmaf(d.x, tt, o.x), fmaf(d.y, tt, o.y), fmaf(d.z, tt, o.z)};
-            } else {
-                const float4 q = pts[g];
-                p = f3{q.x, q.y, q.z};
-            }
+        {
+            float f[kF];
+            encode(p, f);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) store_row8(xs, t, q, kSpX, f + 8 * q);
         }
-        const float s = infer_point(xs, hs, w1s, w2s, tmem, sync, S, b3, p, valid);
-        if (valid && sync.ok) out[g] = s;
+        // the next tile's input is in flight while this tile runs on the tensor cores
+        const uint32_t next = tile + gridDim.x;
+        const uint32_t gn = next * kTile + t;
+        if (next < tiles && gn < total) p = infer_input(pts, rays, origin, dir, interval, gn);
+        float z2[kH];
+        forward_tile(xs, hs, w1s, w2s, tmem, sync, S.b2, z2);
+        float y = b3;
+#pragma unroll
+        for (int o = 0; o < kH; ++o) y += S.w3[o] * fmaxf(z2[o], 0.0f);
+        if (valid && sync.ok) out[g] = softplus(y);
+        tile = next;
+        g = gn;
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, 128);
+    if (warp == 0) tc::tmem_dealloc(tmem, kInferCols);
 }
 
 // ---- coarse-to-fine sampling ---------------------------------------------------------------
 // One warp per ray: coarse opacity a_j = 1 - exp(-s_j L/64), weights T_j a_j, a pdf mixed with
-// 5% uniform, and the 33 fine SDF positions at the CDF quantiles k/32 (t_0 = 0, t_32 = L).
+// the fraction uniform_mix of uniform, and the 33 fine SDF positions at the CDF quantiles k/32
+// (t_0 = 0, t_32 = L).
 __global__ void __launch_bounds__(256) proposal_sample_kernel(const qsdvr_ray_info *__restrict__ rays,
-                                                              uint32_t nrays, float interval,
+                                                              uint32_t nrays, float interval, float uniform_mix,
                                                               const float *__restrict__ dens,
                                                               float *__restrict__ tlist) {
     __shared__ float cdf_s[8][65];
@@ -444,9 +449,9 @@ __global__ void __launch_bounds__(256) proposal_sample_kernel(const qsdvr_ray_in
     float sum = w0 + w1;
 #pragma unroll
     for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
-    const float mix = 0.05f / 64.0f;
-    const float p0 = sum > 0.0f ? 0.95f * w0 / sum + mix : 1.0f / 64.0f;
-    const float p1 = sum > 0.0f ? 0.95f * w1 / sum + mix : 1.0f / 64.0f;
+    const float mix = uniform_mix / 64.0f, keep = 1.0f - uniform_mix;
+    const float p0 = sum > 0.0f ? keep * w0 / sum + mix : 1.0f / 64.0f;
+    const float p1 = sum > 0.0f ? keep * w1 / sum + mix : 1.0f / 64.0f;
     float c = p0 + p1;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -504,25 +509,102 @@ __global__ void __launch_bounds__(256) proposal_targets_kernel(const qsdvr_ray_i
     }
 }
 
-constexpr size_t train_smem() { return kBytesX + kBytesH + 2 * kBytesG + kBytesW1 + kBytesW2 + sizeof(TrainSmem); }
-// At most 4 inference CTAs per SM (4 x 128 TMEM columns): request 52 KiB of shared memory,
-// which is more than the kernel uses, so that a fifth never becomes resident and waits in
-// tcgen05.alloc.  Training CTAs (256 columns) are limited to 2 per SM by their real use.
-constexpr size_t infer_smem() {
-    return kBytesX + kBytesH + kBytesW1 + kBytesW2 + sizeof(InferSmem) > 52 * 1024
-               ? kBytesX + kBytesH + kBytesW1 + kBytesW2 + sizeof(InferSmem)
-               : 52 * 1024;
+// ---- training points drawn straight from the renderer's alphas ----------------------------
+// Point j: a ray r and render sample i < render_count(r) chosen by a counter-based hash of
+// (seed, j) — rays uniformly, then samples uniformly within the ray, up to 16 draws to find a
+// ray with samples — at position midpoint(o, d, i) with target -log(1 - alpha) / interval,
+// alpha read at rays[r].render_offset + i.  A point that finds no such ray gets target -1
+// (ignored by the training kernel).
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {  // a 32-bit finaliser hash
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
 }
 
-unsigned persistent_blocks(const void *fn, size_t smem, uint32_t tiles) {
-    int dev = 0, sms = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, smem);
-    uint64_t b = (uint64_t)sms * (per_sm > 0 ? per_sm : 1);
-    if (b > tiles) b = tiles;
-    return (unsigned)(b ? b : 1);
+__global__ void __launch_bounds__(256) proposal_draw_kernel(const qsdvr_ray_info *__restrict__ rays,
+                                                            const float *__restrict__ origin,
+                                                            const float *__restrict__ dir, uint32_t nrays,
+                                                            float interval, const float *__restrict__ alpha,
+                                                            uint64_t capacity, uint32_t count, uint32_t seed,
+                                                            float4 *__restrict__ pts) {
+    const uint32_t j = blockIdx.x * 256u + threadIdx.x;
+    if (j >= count) return;
+    float4 out = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+    uint32_t h = mix32(j * 0x9e3779b9u ^ mix32(seed));
+    for (int attempt = 0; attempt < 16; ++attempt) {
+        const uint32_t r = (uint32_t)(((uint64_t)h * nrays) >> 32);
+        const qsdvr_ray_info info = rays[r];
+        h = mix32(h + 0x632be5abu);
+        if (info.render_count == 0) continue;
+        const uint32_t i = (uint32_t)(((uint64_t)h * info.render_count) >> 32);
+        const uint64_t m = (uint64_t)info.render_offset + i;
+        if (m >= capacity) {
+            flag_error(QSDVR_DEVERR_CAPACITY);
+            break;
+        }
+        const f3 p = midpoint(load3(origin + 3ull * r), load3(dir + 3ull * r), i, interval);
+        const float a = fminf(fmaxf(alpha[m], 0.0f), 1.0f - 1e-6f);
+        out = make_float4(p.x, p.y, p.z, -log1pf(-a) / interval);
+        break;
+    }
+    pts[j] = out;
 }
+
+constexpr size_t train_smem() { return kBytesX + kBytesH + 2 * kBytesG + kBytesW1 + kBytesW2 + sizeof(TrainSmem); }
+constexpr size_t infer_smem() { return kBytesX + kBytesH + kBytesW1 + kBytesW2 + sizeof(InferSmem); }
+// Shared memory alone keeps every resident CTA's TMEM columns free (2 training CTAs x 256
+// columns, at most 6 inference CTAs x 64), so tcgen05.alloc never has to wait in practice.
+static_assert(2 * train_smem() <= 228 * 1024 && 3 * (train_smem() + 1024) > 228 * 1024,
+              "training CTAs: exactly two per SM");
+static_assert((228 * 1024 / (infer_smem() + 1024)) * kInferCols <= 512, "inference CTAs: TMEM oversubscribed");
+
+// Persistent grid: resident CTAs per SM x SMs, capped at the tile count.  The occupancy API
+// answers 1 CTA per SM for kernels that use tensor memory (it cannot know how many columns a
+// CTA allocates), so residency is computed from the limits themselves: registers (allocated
+// per warp in units of 256), shared memory (plus the per-CTA reservation), threads, and the
+// 512 TMEM columns over the columns each CTA allocates.  Launching that many is safe either
+// way: a CTA whose tcgen05.alloc finds too few free columns waits for a resident CTA to exit,
+// and no CTA waits on another.
+cudaError_t persistent_blocks(const void *fn, size_t smem, uint32_t tmem_cols, uint32_t tiles, unsigned *blocks,
+                              int *per_sm_out) {
+    int dev = 0, sms = 0, regs_sm = 0, smem_sm = 0, reserved = 0, threads_sm = 0, blocks_sm = 0;
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&blocks_sm, cudaDevAttrMaxBlocksPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+    if (e != cudaSuccess) return e;
+    const int warps = kTile / 32;
+    const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
+    int per_sm = regs_sm / (regs_warp * warps);
+    per_sm = min(per_sm, smem_sm / (int)(smem + fa.sharedSizeBytes + reserved));
+    per_sm = min(per_sm, threads_sm / kTile);
+    per_sm = min(per_sm, blocks_sm);
+    per_sm = min(per_sm, (int)(512 / tmem_cols));
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t b = (uint64_t)sms * (uint64_t)per_sm;
+    if (b > tiles) b = tiles;
+    *blocks = (unsigned)(b ? b : 1);
+    if (per_sm_out) *per_sm_out = per_sm;
+    return cudaSuccess;
+}
+
+// Opt each kernel in to its dynamic shared memory once per process.
+int configure(const void *fn, size_t smem, bool *done, const char *what) {
+    if (*done) return QSDVR_OK;
+    const int st = check_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), what);
+    if (st == QSDVR_OK) *done = true;
+    return st;
+}
+
+bool g_train_configured = false, g_infer_configured = false;
 
 }  // namespace
 }  // namespace qsdvr
@@ -536,20 +618,16 @@ extern "C" int qsdvr_mlp_train(const float *points, uint32_t count, const void *
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_mlp_train: null pointer");
     if (!aligned(points, 16) || !aligned(params_bf16, 16))
         return set_error(QSDVR_ERR_ALIGNMENT, "qsdvr_mlp_train: points and params need 16-byte alignment");
-    const size_t smem = train_smem();
-    static bool configured = false;
-    if (!configured) {
-        const int st = check_cuda(
-            cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-            "qsdvr_mlp_train: smem attribute");
-        if (st != QSDVR_OK) return st;
-        configured = true;
-    }
-    const uint32_t tiles = (count + kTile - 1) / kTile;
-    const unsigned blocks = persistent_blocks((const void *)mlp_train_kernel, smem, tiles);
-    mlp_train_kernel<<<blocks, 128, smem, stream>>>(reinterpret_cast<const float4 *>(points), count,
-                                                    static_cast<const __nv_bfloat16 *>(params_bf16), under_weight,
-                                                    grad, loss);
+    const void *fn = (const void *)mlp_train_kernel;
+    int st = configure(fn, train_smem(), &g_train_configured, "qsdvr_mlp_train: smem attribute");
+    if (st != QSDVR_OK) return st;
+    unsigned blocks = 0;
+    st = check_cuda(persistent_blocks(fn, train_smem(), kTrainCols, (count + kTile - 1) / kTile, &blocks, nullptr),
+                    "qsdvr_mlp_train: occupancy");
+    if (st != QSDVR_OK) return st;
+    mlp_train_kernel<<<blocks, kTile, train_smem(), stream>>>(reinterpret_cast<const float4 *>(points), count,
+                                                              static_cast<const __nv_bfloat16 *>(params_bf16),
+                                                              under_weight, grad, loss);
     return check_launch("qsdvr_mlp_train");
 }
 
@@ -564,29 +642,45 @@ extern "C" int qsdvr_mlp_density(const float *points, uint32_t count, const qsdv
         return set_error(QSDVR_ERR_ALIGNMENT, "qsdvr_mlp_density: points and params need 16-byte alignment");
     if (rays && ray_count > (1u << 25))
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_mlp_density: too many rays");
-    const size_t smem = infer_smem();
-    static bool configured = false;
-    if (!configured) {
-        const int st = check_cuda(
-            cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-            "qsdvr_mlp_density: smem attribute");
-        if (st != QSDVR_OK) return st;
-        configured = true;
-    }
-    const uint32_t tiles = (total + kTile - 1) / kTile;
-    const unsigned blocks = persistent_blocks((const void *)mlp_infer_kernel, smem, tiles);
-    mlp_infer_kernel<<<blocks, 128, smem, stream>>>(reinterpret_cast<const float4 *>(points), count, rays, origin, dir,
-                                                    ray_count, interval,
-                                                    static_cast<const __nv_bfloat16 *>(params_bf16), out);
+    const void *fn = (const void *)mlp_infer_kernel;
+    int st = configure(fn, infer_smem(), &g_infer_configured, "qsdvr_mlp_density: smem attribute");
+    if (st != QSDVR_OK) return st;
+    unsigned blocks = 0;
+    st = check_cuda(persistent_blocks(fn, infer_smem(), kInferCols, (total + kTile - 1) / kTile, &blocks, nullptr),
+                    "qsdvr_mlp_density: occupancy");
+    if (st != QSDVR_OK) return st;
+    mlp_infer_kernel<<<blocks, kTile, infer_smem(), stream>>>(reinterpret_cast<const float4 *>(points), count, rays,
+                                                              origin, dir, ray_count, interval,
+                                                              static_cast<const __nv_bfloat16 *>(params_bf16), out);
     return check_launch("qsdvr_mlp_density");
 }
 
+extern "C" int qsdvr_mlp_launch_shape(int kernel, uint32_t count, uint32_t *blocks, int *blocks_per_sm) {
+    if (!blocks || !blocks_per_sm || (kernel != 0 && kernel != 1))
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_mlp_launch_shape: bad arguments");
+    const void *fn = kernel == 0 ? (const void *)mlp_infer_kernel : (const void *)mlp_train_kernel;
+    const size_t smem = kernel == 0 ? infer_smem() : train_smem();
+    int st = configure(fn, smem, kernel == 0 ? &g_infer_configured : &g_train_configured,
+                       "qsdvr_mlp_launch_shape: smem attribute");
+    if (st != QSDVR_OK) return st;
+    unsigned b = 0;
+    st = check_cuda(persistent_blocks(fn, smem, kernel == 0 ? kInferCols : kTrainCols, (count + kTile - 1) / kTile, &b,
+                                      blocks_per_sm),
+                    "qsdvr_mlp_launch_shape: occupancy");
+    *blocks = b;
+    return st;
+}
+
 extern "C" int qsdvr_proposal_sample(const qsdvr_ray_info *rays, uint32_t ray_count, float interval,
-                                     const float *coarse_density, float *tlist, cudaStream_t stream) {
+                                     float uniform_mix, const float *coarse_density, float *tlist,
+                                     cudaStream_t stream) {
     if (ray_count == 0) return QSDVR_OK;
     if (!rays || !coarse_density || !tlist)
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_proposal_sample: null pointer");
-    proposal_sample_kernel<<<grid_for(ray_count, 8), 256, 0, stream>>>(rays, ray_count, interval, coarse_density, tlist);
+    if (!(uniform_mix > 0.0f && uniform_mix <= 1.0f))
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_proposal_sample: uniform_mix must be in (0, 1]");
+    proposal_sample_kernel<<<grid_for(ray_count, 8), 256, 0, stream>>>(rays, ray_count, interval, uniform_mix,
+                                                                       coarse_density, tlist);
     return check_launch("qsdvr_proposal_sample");
 }
 
@@ -600,4 +694,17 @@ extern "C" int qsdvr_proposal_targets(const qsdvr_ray_info *rays, const float *o
     proposal_targets_kernel<<<grid_for((uint64_t)ray_count * 32, 256), 256, 0, stream>>>(
         rays, origin, dir, ray_count, interval, alpha, sample_count, reinterpret_cast<float4 *>(points));
     return check_launch("qsdvr_proposal_targets");
+}
+
+extern "C" int qsdvr_proposal_draw(const qsdvr_ray_info *rays, const float *origin, const float *dir,
+                                   uint32_t ray_count, float interval, const float *alpha, uint64_t sample_count,
+                                   uint32_t count, uint32_t seed, float *points, cudaStream_t stream) {
+    if (count == 0) return QSDVR_OK;
+    if (ray_count == 0 || !rays || !origin || !dir || !alpha || !points)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_proposal_draw: null pointer or no rays");
+    if (!aligned(points, 16)) return set_error(QSDVR_ERR_ALIGNMENT, "qsdvr_proposal_draw: points alignment");
+    proposal_draw_kernel<<<grid_for(count, 256), 256, 0, stream>>>(rays, origin, dir, ray_count, interval, alpha,
+                                                                  sample_count, count, seed,
+                                                                  reinterpret_cast<float4 *>(points));
+    return check_launch("qsdvr_proposal_draw");
 }

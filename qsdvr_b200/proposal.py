@@ -26,9 +26,14 @@ N_FINE_T = 33
 _lib.extra_signatures({
     "qsdvr_mlp_density": [P, U32, P, P, P, U32, F32, P, P, P],
     "qsdvr_mlp_train": [P, U32, P, F32, P, P, P],
-    "qsdvr_proposal_sample": [P, U32, F32, P, P, P],
+    "qsdvr_proposal_sample": [P, U32, F32, F32, P, P, P],
     "qsdvr_proposal_targets": [P, P, P, U32, F32, P, U64, P, P],
+    "qsdvr_proposal_draw": [P, P, P, U32, F32, P, U64, U32, U32, P, P],
+    "qsdvr_mlp_launch_shape": [ctypes.c_int, U32, P, P],
 })
+
+INFER_MIX = 0.05  # uniform share of the fine-sample pdf when rendering
+TRAIN_MIX = 0.25  # and when training the grid at the proposal's samples
 
 
 def _p(t):
@@ -64,6 +69,7 @@ class ProposalNet:
         self.step_count = 0
         self.lr = lr
         self.under_weight = under_weight
+        self._bufs: dict = {}
 
     # ---- inference
     def density(self, points: torch.Tensor) -> torch.Tensor:
@@ -85,9 +91,9 @@ class ProposalNet:
              _p(self.params_bf16), _p(out), _stream(self.device))
         return out
 
-    def sample(self, rays, origin, direction, interval) -> torch.Tensor:
+    def sample(self, rays, origin, direction, interval, uniform_mix: float = INFER_MIX) -> torch.Tensor:
         """[N, 33] fine SDF positions (t from each ray's origin) from 64 coarse evaluations."""
-        return sample_fine(rays, interval, self.coarse_density(rays, origin, direction, interval))
+        return sample_fine(rays, interval, self.coarse_density(rays, origin, direction, interval), uniform_mix)
 
     def render(self, rays, origin, direction, sdf_grid, data, reso, interval, k, mode="fixed",
                transmittance="product"):
@@ -111,26 +117,47 @@ class ProposalNet:
         adam_step(self.params, self.grad, self.m, self.v, self.step_count, self.lr, param_bf16=self.params_bf16)
         return loss
 
+    def _buffer(self, name, shape, dtype):
+        buf = self._bufs.get(name)
+        if buf is None or buf.shape != shape:
+            buf = torch.empty(shape, dtype=dtype, device=self.device)
+            self._bufs[name] = buf
+        return buf
+
     def online_step(self, rays, origin, direction, sdf_grid, data, reso, interval, k, mode="fixed",
-                    transmittance="product", points: int = 65536, generator=None):
+                    transmittance="product", points: int = 65536, seed: int | None = None):
         """Online training from the renderer: a uniform-march forward over ``rays`` writes each
-        render sample's alpha, which become (position, density) targets; one Adam step on
-        ``points`` of them drawn at random.  No host synchronisation."""
-        _, r, alpha, total = uniform_alpha(rays, origin, direction, sdf_grid, data, reso, interval, k, mode,
-                                           transmittance)
-        pts = targets(r, origin, direction, interval, alpha)
-        u = torch.rand(points, device=rays.device, generator=generator)
-        idx = torch.clamp((u * total).long(), max=pts.shape[0] - 1)
-        return self.train_step(pts[idx].contiguous())
+        render sample's alpha (ray r's samples at r * stride), ``points`` of them are drawn at
+        random as (position, density) targets, and one Adam step follows.  Five launches, no
+        host synchronisation."""
+        n = rays.shape[0]
+        stride = max_render_samples(interval)
+        off = self._bufs.get(("offsets", n, stride))
+        if off is None:
+            off = torch.arange(0, n * stride, stride, dtype=torch.int32, device=self.device)
+            self._bufs[("offsets", n, stride)] = off
+        r = self._buffer("rays", (n, 4), torch.int32)
+        r.copy_(rays)
+        r[:, 3] = off
+        alpha = self._buffer("alpha", (n * stride,), torch.float32)
+        fused.render_forward(r, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance,
+                             sample_alpha=alpha)
+        pts = self._buffer("points", (points, 4), torch.float32)
+        seed = self.step_count if seed is None else seed
+        call("qsdvr_proposal_draw", _p(r), _p(origin), _p(direction), n, float(interval), _p(alpha), alpha.numel(),
+             points, int(seed) & 0xFFFFFFFF, _p(pts), _stream(self.device))
+        return self.train_step(pts)
 
 
-def sample_fine(rays, interval, coarse) -> torch.Tensor:
-    """[N, 33] fine SDF positions from [N, 64] coarse densities (inverse-CDF sampling)."""
+def sample_fine(rays, interval, coarse, uniform_mix: float = INFER_MIX) -> torch.Tensor:
+    """[N, 33] fine SDF positions from [N, 64] coarse densities (inverse-CDF sampling of the
+    coarse compositing weights mixed with ``uniform_mix`` of a uniform density)."""
     if coarse.dtype != torch.float32 or coarse.shape != (rays.shape[0], N_COARSE) or not coarse.is_contiguous():
         raise ValueError("coarse must be a contiguous float32 [N, 64] tensor")
     n = rays.shape[0]
     t = torch.empty((n, N_FINE_T), dtype=torch.float32, device=rays.device)
-    call("qsdvr_proposal_sample", _p(rays), n, float(interval), _p(coarse), _p(t), _stream(rays.device))
+    call("qsdvr_proposal_sample", _p(rays), n, float(interval), float(uniform_mix), _p(coarse), _p(t),
+         _stream(rays.device))
     return t
 
 

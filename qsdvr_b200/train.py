@@ -67,6 +67,7 @@ def parser():
     ap.add_argument("--proposal-rays", type=int, default=4096, help="rays of the per-step uniform pass")
     ap.add_argument("--proposal-points", type=int, default=65536, help="MLP training points per step")
     ap.add_argument("--proposal-lr", type=float, default=5e-3)
+    ap.add_argument("--proposal-mix", type=float, default=0.25, help="uniform share of the fine-sample pdf")
     ap.add_argument("--log-every", type=int, default=100)
     ap.add_argument("--seed", type=int, default=0)
     return ap
@@ -95,7 +96,6 @@ def run(a, data=None, quiet=False):
     model.sdfGrid.grad = torch.zeros_like(model.sdfGrid)
     model.renderData.grad = torch.zeros_like(model.renderData)
     net = ProposalNet(dev, seed=a.seed, lr=a.proposal_lr) if a.proposal else None
-    pgen = torch.Generator(device=dev).manual_seed(a.seed + 2)
     loss = torch.zeros(1, dtype=torch.float32, device=dev)
     log = []
 
@@ -127,8 +127,8 @@ def run(a, data=None, quiet=False):
         if net is not None:
             n = min(a.proposal_rays, a.rays)
             net.online_step(r[:n], o[:n], d[:n], sg, dg, R, a.interval, a.k, a.mode, model.transmittance,
-                            points=a.proposal_points, generator=pgen)
-            tlist = net.sample(r, o, d, a.interval)
+                            points=a.proposal_points)
+            tlist = net.sample(r, o, d, a.interval, a.proposal_mix)
         fused.render_train(tg, r, o, d, sg, dg, R, a.interval, a.k, model.sdfGrid.grad, model.renderData.grad,
                            a.mode, model.transmittance, loss=loss, tlist=tlist)
         e1.record()

@@ -44,6 +44,7 @@ def _points(n, seed=1):
     p = np.zeros((n, 4), np.float32)
     p[:, :3] = g.uniform(-1, 1, (n, 3))
     p[:, 3] = g.exponential(2.0, n) * (g.uniform(0, 1, n) < 0.5)
+    p[g.uniform(0, 1, n) < 0.1, 3] = -1.0  # ignored points
     return p
 
 
@@ -57,6 +58,21 @@ def _net(prop, w):
 def _close(got, want, atol, rtol):
     got, want = np.asarray(got, np.float64), np.asarray(want, np.float64)
     return float(np.max(np.abs(got - want) / (atol + rtol * np.abs(want))))
+
+
+def test_mlp_kernels_fill_the_gpu(prop):
+    """The persistent MLP kernels run as many CTAs per SM as registers, shared memory and
+    tensor memory allow (inference: 5 of 64 TMEM columns each; training: 2 of 256)."""
+    import ctypes
+
+    from qsdvr_b200._lib import call
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    for kernel, want in ((0, 5), (1, 2)):
+        blocks, per_sm = ctypes.c_uint32(), ctypes.c_int()
+        call("qsdvr_mlp_launch_shape", kernel, 1 << 24, ctypes.byref(blocks), ctypes.byref(per_sm))
+        print(f"kernel {kernel}: {per_sm.value} CTAs/SM, grid {blocks.value}")
+        assert per_sm.value == want and blocks.value == want * sms
 
 
 @pytest.mark.parametrize("n", [1, 200, 5000])
@@ -113,10 +129,12 @@ def test_proposal_sample_vs_oracle(prop):
     dens[5] = 0.0
     dens[6, 10] = 5e3
     interval = 4.0 / 256
-    got = prop.sample_fine(torch.from_numpy(rays).to(DEV), interval, torch.from_numpy(dens).to(DEV)).cpu().numpy()
-    want = OP.sample(rays, interval, dens)
-    assert np.abs(got - want).max() < 2e-4
-    assert np.all(np.diff(got, axis=1) >= 0.0)
+    for mix in (0.05, 0.25, 1.0):
+        got = prop.sample_fine(torch.from_numpy(rays).to(DEV), interval, torch.from_numpy(dens).to(DEV),
+                               mix).cpu().numpy()
+        want = OP.sample(rays, interval, dens, mix)
+        assert np.abs(got - want).max() < 2e-4
+        assert np.all(np.diff(got, axis=1) >= 0.0)
 
 
 def test_proposal_targets_vs_oracle(prop):
@@ -139,6 +157,60 @@ def test_proposal_targets_vs_oracle(prop):
     want = OP.targets(rays, origin, d, interval, alpha)
     assert np.abs(got[:, :3] - want[:, :3]).max() < 1e-6
     assert _close(got[:, 3], want[:, 3], 1e-3, 1e-4) <= 1.0
+
+
+def test_proposal_draw_picks_real_samples(prop):
+    """Every drawn point is one of the batch's render samples with its density target; rays
+    without samples are never drawn; rays are hit about uniformly."""
+    from qsdvr_b200._lib import call
+
+    rng = np.random.default_rng(8)
+    n, stride = 200, 50
+    rays = np.zeros((n, 4), np.int32)
+    rays[:, 0] = rng.integers(0, 40, n)
+    rays[:, 0][rays[:, 0] == 1] = 0
+    rays[:, 2] = np.maximum(rays[:, 0] - 1, 0)
+    rays[:, 3] = np.arange(n) * stride
+    origin = rng.uniform(-0.9, 0.9, (n, 3)).astype(np.float32)
+    d = rng.standard_normal((n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    alpha = rng.uniform(0, 0.9, n * stride).astype(np.float32)
+    interval = 0.02
+    dev = [torch.from_numpy(a).to(DEV) for a in (rays, origin, d, alpha)]
+    count = 20000
+    pts = torch.empty((count, 4), device=DEV)
+    call("qsdvr_proposal_draw", dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr(), n, interval,
+         dev[3].data_ptr(), n * stride, count, 1234, pts.data_ptr(), None)
+    from scipy.spatial import cKDTree
+
+    got = pts.cpu().numpy().astype(np.float64)
+    want = OP.targets(rays, origin, d, interval, alpha)
+    rows = np.concatenate([np.arange(r * stride, r * stride + rays[r, 2]) for r in range(n)])
+    dist, nearest = cKDTree(want[rows, :3]).query(got[:, :3])
+    assert dist.max() < 1e-5 and (got[:, 3] >= 0.0).all()
+    m = rows[nearest]
+    assert np.all(np.abs(got[:, 3] - want[m, 3]) <= 1e-3 + 1e-4 * want[m, 3])
+    hits = np.bincount(m // stride, minlength=n)
+    has = rays[:, 2] > 0
+    assert not hits[~has].any()
+    expect = count / has.sum()
+    assert hits[has].min() > 0.6 * expect and hits[has].max() < 1.5 * expect
+
+
+def test_online_step_fits_the_renderer(prop):
+    """Online training (uniform-march alphas of the batch -> drawn points -> Adam) lowers the
+    loss on a scene's density."""
+    from qsdvr_b200 import fused, scenes
+
+    R, k, interval = 48, 20.0, 4.0 / 256
+    grid8 = fused.pad_grid7(scenes.sphere_grid(R, 0.5, 0.0, device=DEV).reshape(-1, 7))
+    data = scenes.appearance(R, seed=0, device=DEV)
+    cam = _camera((3.0, 2.0, 1.5), 64, 88.9, interval, R)
+    net = prop.ProposalNet(DEV, seed=1)
+    losses = [float(net.online_step(cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k,
+                                    points=16384)) for _ in range(300)]
+    assert np.mean(losses[-20:]) < 0.3 * np.mean(losses[:5])
+    assert net.step_count == 300
 
 
 def _camera(pos, size, focal, interval, R):
