@@ -47,7 +47,12 @@ WORKLOADS = {
                          storage="bf16", sh=3),
     "sh3_128": dict(R=128, rays=8192, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
                     storage="f32", sh=3),
+    # learned proposal form: full-frame renders of a trained 384^3 BF16 SH3 model, 64 coarse MLP
+    # points + 32 fine samples per ray against the 512-sample uniform march
+    "proposal384": dict(R=384, rays=65536, views=200, size=800, focal=1111.1, radius=4.03, interval=4.0 / 512,
+                        storage="bf16", sh=3, train_steps=200, heldout=4),
 }
+PROPOSAL_STEPS = 300  # training steps per method in the default line's proposal comparison
 
 
 def bytes_per_sample(storage: str, sh: int) -> int:
@@ -342,7 +347,120 @@ def run_ours(args, cfg, device, ws, rank):
     }
     if ws == 1 and not args.no_cpu_baseline and cfg.get("sh", 2) == 2:  # the reference's CPU path is SH degree 2
         out["cpu_baseline"] = cpu_baseline(scene, batches[0], cfg, args.cpu_rays)
+    if ws == 1 and args.workload == "plain256" and not args.no_proposal:
+        del scene, batches
+        torch.cuda.empty_cache()
+        out["proposal"] = proposal_comparison(PROPOSAL_STEPS)
     return out
+
+
+# ----------------------------------------------------------------------------- proposal path
+
+def proposal_comparison(steps: int):
+    """Training at 256^3 with each method from the same initial model on the same batches:
+    the uniform march (256 samples/ray) and the proposal network (64 coarse MLP points + 32
+    fine samples/ray, trained online).  rays/s is device time of the forward + backward part of
+    the steps (for the proposal: coarse MLP, sampler, online network update and the fused
+    train launch); PSNR is on 65536 held-out rays, judged by the uniform march."""
+    from qsdvr_b200 import train
+
+    a = train.parser().parse_args([])
+    a.steps, a.log_every = steps, 10 ** 9
+    data = train.build(a.reso, a.views, a.size, 1111.1 * a.size / 800, 4.03, a.interval, a.k, a.seed,
+                       torch.device("cuda", torch.cuda.current_device()))
+    plain = train.run(a, data, quiet=True)
+    a.proposal = True
+    prop = train.run(a, data, quiet=True)
+    del data
+    torch.cuda.empty_cache()
+    return {"method": "64 coarse MLP points + 32 fine samples per ray (tcgen05 MLP, trained online)",
+            "workload": f"R={a.reso}^3 fp32 fixed mode, {a.rays} rays/step, {steps} training steps per method from "
+                        f"the same sphere init, k={a.k}, Adam lr {a.lr}",
+            "train_rays_per_s": prop["render_rays_per_s"], "plain_train_rays_per_s": plain["render_rays_per_s"],
+            "speedup": round(prop["render_rays_per_s"] / plain["render_rays_per_s"], 3),
+            "render_ms_per_step": round(prop["render_ms"] / steps, 4),
+            "plain_render_ms_per_step": round(plain["render_ms"] / steps, 4),
+            "optimizer_ms_per_step": round(prop["optimizer_ms"] / steps, 4),
+            "psnr_plain": plain["heldout_psnr_end"], "psnr_proposal": prop["heldout_psnr_end"],
+            "delta_psnr": round(plain["heldout_psnr_end"] - prop["heldout_psnr_end"], 3),
+            "judge": "held-out rays rendered with the 256-sample uniform march vs ground truth"}
+
+
+def run_proposal_frames(args, cfg, device):
+    """Learned proposal form: train a BF16 SH3 model (uniform march, proposal network trained
+    online beside it), then render held-out full frames with the 512-sample uniform march and
+    with 64 coarse MLP points + 32 fine samples per ray; rays/s (all pixels) and PSNR of each
+    against the ground-truth frames."""
+    from qsdvr_b200 import fused, scenes, train
+    from qsdvr_b200.camera import Camera
+
+    R, interval = cfg["R"], cfg["interval"]
+    a = train.parser().parse_args([])
+    a.reso, a.interval, a.sh, a.storage, a.views = R, interval, cfg["sh"], cfg["storage"], cfg["views"]
+    a.steps, a.rays, a.log_every, a.online_proposal = cfg["train_steps"], cfg["rays"], 10 ** 9, True
+    size = cfg["size"]
+    data = train.build(R, a.views, size, cfg["focal"], cfg["radius"], interval, a.k, a.seed, device, a.sh)
+    summary, model, net = train.run(a, data, quiet=True, return_state=True)
+    del data
+    torch.cuda.empty_cache()
+    # held-out views (a different camera seed) and their ground truth from the uniform march
+    gt_sdf = fused.pad_grid7(scenes.procedural_grid(R, seed=a.seed, device=device).reshape(-1, 7))
+    gt_data = scenes.appearance(R, seed=a.seed, device=device, procedural=True, sh_degree=a.sh)
+    frames = []
+    for cam in scenes.hemisphere_cameras(cfg["heldout"], cfg["radius"], size, size, cfg["focal"], 2.0, 6.0,
+                                         seed=a.seed + 99):
+        c = Camera(cam, interval, R, device=device)
+        c.GenerateRayPoints(torch.ones(size * size, dtype=torch.bool))
+        gt = fused.render_forward(c.rayList, c.originList, c.dirList, gt_sdf, gt_data, R, interval, a.k, "fixed")
+        frames.append((c.rayList, c.originList, c.dirList, gt))
+    del gt_sdf, gt_data
+    torch.cuda.empty_cache()
+    sg, dg = model.grids()
+    sg, dg = sg.detach(), dg.detach()
+    stream = torch.cuda.current_stream(device)
+
+    def uniform(f):
+        return fused.render_forward(f[0], f[1], f[2], sg, dg, R, interval, a.k, "fixed", model.transmittance)
+
+    def proposal(f):
+        return net.render(f[0], f[1], f[2], sg, dg, R, interval, a.k, "fixed", model.transmittance)
+
+    out = {}
+    for name, fn in (("uniform", uniform), ("proposal", proposal)):
+        mse = sum(float(((fn(f) - f[3]) ** 2).mean()) for f in frames) / len(frames)
+
+        def step(i, ev, fn=fn):
+            if ev is not None:
+                ev[0].record(stream)
+            fn(frames[i % len(frames)])
+            if ev is not None:
+                ev[1].record(stream)
+
+        with ClockSampler(device.index) as clk:
+            time.sleep(0.3)
+            total_ms, kern_ms = time_device(step, args.steps, args.warmup, stream, clk)
+        out[name] = dict(ms_per_frame=total_ms / args.steps, psnr=-10.0 * np.log10(max(mse, 1e-12)),
+                         clocks=clk.summary())
+    pixels = size * size
+    value = pixels / (out["proposal"]["ms_per_frame"] / 1e3)
+    plain = pixels / (out["uniform"]["ms_per_frame"] / 1e3)
+    return {
+        "metric": "full-frame render rays/s, proposal (64 coarse + 32 fine) vs 512-sample uniform march",
+        "value": round(value, 1), "unit": "rays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(out["proposal"]["ms_per_frame"], 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 storage, f32 math; MLP bf16 with f32 accumulation",
+        "data": "synthetic (seeded procedural scene; model trained from a sphere init)",
+        "config": {"workload": f"proposal384: R={R}^3 BF16 SH3 model after {a.steps} training steps "
+                               f"({a.rays} rays/step, uniform 512 march, proposal network trained online), "
+                               f"{cfg['heldout']} held-out {size}^2 frames, k={a.k}",
+                   "global_batch": pixels, "step": "one full frame (all pixels, hit or not)",
+                   "l2": "grids 8.2 GB, larger than L2; no flush", "parallelism": "replicas x1"},
+        "plain_value": round(plain, 1), "speedup": round(value / plain, 3),
+        "psnr_uniform512": round(out["uniform"]["psnr"], 3), "psnr_proposal": round(out["proposal"]["psnr"], 3),
+        "delta_psnr": round(out["uniform"]["psnr"] - out["proposal"]["psnr"], 3),
+        "train_summary": {k: summary[k] for k in ("heldout_psnr_end", "ms_per_step", "peak_memory_gb")},
+        "gpu_launches": 3 * args.steps, "clocks": out["proposal"]["clocks"],
+    }
 
 
 # ----------------------------------------------------------------------------- CPU path
@@ -442,6 +560,7 @@ def main():
     ap.add_argument("--workload", default="plain256", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-rays", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-proposal", action="store_true", help="skip the proposal-path comparison")
     ap.add_argument("--views", type=int, default=None, help="override the number of camera views (ray pool size)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -462,6 +581,11 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=device)
     try:
+        if args.workload == "proposal384":
+            if ws > 1:
+                raise SystemExit("proposal384 is a single-GPU workload")
+            print(json.dumps(run_proposal_frames(args, cfg, device)))
+            return
         out = run_ours(args, cfg, device, ws, rank)
         if rank == 0:
             print(json.dumps(out))

@@ -43,7 +43,9 @@ enum {
     QSDVR_DEVERR_TIMEOUT = 8u       /* a bounded wait on the tensor cores gave up       */
 };
 
-/* Shading / indexing modes. */
+/* Shading / indexing modes.  In the fused renderer, fixed mode also computes alpha and its
+ * derivatives in an overflow-free form (softplus of -k sdf) and treats an SDF sample where
+ * the cell's quadric is degenerate (|grad f|^2 < 1e-30 or |sdf| > 4) as empty. */
 enum {
     QSDVR_MODE_COMPAT = 0, /* the reference exactly: overlapping SH reads, sheared vertex index */
     QSDVR_MODE_FIXED = 1   /* packed SH layout, vertex index x + y(R+1) + z(R+1)^2             */
@@ -294,8 +296,8 @@ int qsdvr_render_loss_f64(const qsdvr_ray_info *rays, const float *origin, const
 #define QSDVR_MLP_PARAMS 6280
 
 /* Density bound at points [count][4] (x, y, z, ignored), or, when rays is not null, at the
- * 64 coarse points t = (j + 0.5) L / 64 of every ray (L = (sdf_count - 1) interval); out is
- * [count] or [ray_count][64]. */
+ * 64 coarse points t = (j + 0.5) L / 64 of every ray (L = (sdf_count - 1) interval; rays
+ * with sdf_count < 2 get 0); out is [count] or [ray_count][64]. */
 int qsdvr_mlp_density(const float *points, uint32_t count, const qsdvr_ray_info *rays, const float *origin,
                       const float *dir, uint32_t ray_count, float interval, const void *params_bf16, float *out,
                       cudaStream_t stream);

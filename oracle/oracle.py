@@ -200,6 +200,21 @@ def sample_sdf(grid7: torch.Tensor, points: torch.Tensor, index: torch.Tensor, r
     return value / norm / reso
 
 
+MAX_SDF, MIN_GRAD2 = 4.0, 1e-30
+
+
+def sdf_trusted(grid7: torch.Tensor, points: torch.Tensor, index: torch.Tensor, reso: float):
+    """fixed mode's rule for a usable SDF sample (qsdvr_b200/csrc/fused.cu checked_sdf): |grad f|^2
+    at least 1e-30 and |sdf| at most 4 (a degenerate quadric point otherwise); no counterpart
+    in the reference."""
+    with torch.no_grad():
+        g = grid7.reshape(-1, 7)[_t(index).long()]
+        p = _t(points).to(g.dtype)
+        len2 = sum((2 * g[:, c] * p[:, c] + g[:, 3 + c]) ** 2 for c in range(3))
+        sdf = sample_sdf(grid7, points, index, reso)
+        return torch.isfinite(sdf) & (sdf.abs() <= MAX_SDF) & (len2 >= MIN_GRAD2)
+
+
 def sample_normal(grid7: torch.Tensor, points: torch.Tensor, index: torch.Tensor):
     """kernel/surface.cu:104-115: normalize(2 a_k u_k + a_{k+3})."""
     g = grid7.reshape(-1, 7)[_t(index).long()]
@@ -399,15 +414,19 @@ def _ray_matrix(rays: torch.Tensor):
     return valid, r_idx, s0
 
 
-def ray_aggregate(rgb, sdf, rays, k: float):
+def ray_aggregate(rgb, sdf, rays, k: float, sdf_ok=None):
     """kernel/render.cu:223-253: NeuS alpha and front-to-back compositing per ray.
 
     E_i = exp(-k sdf_i); alpha_i = max((E_{i+1} - E_i) / (1 + E_{i+1}), 0);
     T_0 = 1, T_{i+1} = T_i (1 - alpha_i); C = sum_i T_i alpha_i rgb_i.
+    ``sdf_ok`` (fixed mode): intervals with an untrusted end sample are empty (alpha 0).
     Returns (color [N,3], alpha [M], T [M]) with alpha/T at each render sample.
     """
     rgb, sdf = _t(rgb), _t(sdf)
     valid, r_idx, s0 = _ray_matrix(rays)
+    if sdf_ok is not None:
+        valid = valid & sdf_ok[s0] & sdf_ok[s0 + valid.long()]
+        sdf = torch.where(sdf_ok, sdf, torch.zeros_like(sdf))
     E0 = torch.exp(-k * sdf[s0])
     E1 = torch.exp(-k * sdf[s0 + valid.long()])
     x = (E1 - E0) / (1.0 + E1)
@@ -480,6 +499,7 @@ def render(sdf_grid7, data, inputs: dict, k: float, compat: bool = True, sh_degr
     g7 = sdf_grid7.reshape(-1, 7)
     R = round(g7.shape[0] ** (1.0 / 3.0))
     sdf = sample_sdf(g7, inputs["sdfPointList"], inputs["sdfIndexList"], R)
+    sdf_ok = None if compat else sdf_trusted(g7, inputs["sdfPointList"], inputs["sdfIndexList"], R)
     normal = sample_normal(g7, inputs["renderPointList"], inputs["renderIndexList"])
     vidx = vertex_index(inputs["renderIndexList"], R, compat)
     d = grid_interpolation(data.reshape(-1, data.shape[-1]), inputs["renderPointList"], vidx, R + 1)
@@ -487,5 +507,5 @@ def render(sdf_grid7, data, inputs: dict, k: float, compat: bool = True, sh_degr
         rgb = shader_sh3(normal, _t(inputs["viewDirList"]).to(DTYPE), d)
     else:
         rgb = shade(normal, _t(inputs["viewDirList"]).to(DTYPE), d, compat)
-    color, _, _ = ray_aggregate(rgb, sdf, inputs["rayList"], k)
+    color, _, _ = ray_aggregate(rgb, sdf, inputs["rayList"], k, sdf_ok)
     return color

@@ -169,35 +169,84 @@ __device__ __forceinline__ bool cell_in_grid(const CellPoint &c, uint32_t R) {
     return (unsigned)c.cx < R && (unsigned)c.cy < R && (unsigned)c.cz < R;
 }
 
-// alpha of one interval (kernel/render.cu:244).  compat: the reference's expression.
-// fixed: the same value, with the limits taken where exp(-k sdf) overflows (alpha -> 1 when
-// only the far end overflows, 0 when both do) instead of inf/inf.
+// The two per-sample terms of an interval's alpha.  compat: E = exp(-k sdf), the
+// reference's (kernel/render.cu:239-244).  fixed: L = softplus(-k sdf) = -log sigmoid(k sdf),
+// finite for every finite sdf, so no intermediate overflows however deep a sample lies.
 template <bool kCompat>
-__device__ __forceinline__ float interval_alpha(float e0, float e1) {
-    if (!kCompat && isinf(e1)) return isinf(e0) ? 0.0f : 1.0f;
-    return fmaxf((e1 - e0) / (1.0f + e1), 0.0f);
+__device__ __forceinline__ float alpha_term(float k, float sdf) {
+    const float x = -k * sdf;
+    if (kCompat) return expf(x);
+    return fmaxf(x, 0.0f) + log1pf(expf(-fabsf(x)));
 }
 
-// d alpha / d sdf_{i+1} and d alpha / d sdf_i (kernel/render.cu:271-273).  fixed mode uses
-// q = 1 / (1 + e1), e1 q = 1 - q, which stays finite (and tends to 0) when e1 overflows.
+// alpha of one interval (kernel/render.cu:244).  compat: the reference's expression
+// max((E1 - E0) / (1 + E1), 0).  fixed: the same quantity 1 - sigmoid(k s1) / sigmoid(k s0)
+// = -expm1(L0 - L1), clamped at 0.
 template <bool kCompat>
-__device__ __forceinline__ void interval_dalpha(float e0, float e1, float k, float *d_next, float *d_this) {
+__device__ __forceinline__ float interval_alpha(float t0, float t1) {
+    if (kCompat) return fmaxf((t1 - t0) / (1.0f + t1), 0.0f);
+    return t0 < t1 ? -expm1f(t0 - t1) : 0.0f;
+}
+
+// d alpha / d sdf_{i+1} and d alpha / d sdf_i where alpha > 0 (kernel/render.cu:271-273).
+// fixed: with 1 - alpha = exp(L0 - L1) and sigmoid(-k s) = -expm1(-L),
+//   d alpha / d s0 = (1 - alpha) k sigmoid(-k s0),  d alpha / d s1 = -(1 - alpha) k sigmoid(-k s1),
+// both bounded by k.
+template <bool kCompat>
+__device__ __forceinline__ void interval_dalpha(float t0, float t1, float k, float *d_next, float *d_this) {
     if (kCompat) {
-        const float inv = 1.0f / (1.0f + e1);
-        *d_next = -k * e1 * (1.0f + e0) * inv * inv;
-        *d_this = k * e0 * inv;
+        const float inv = 1.0f / (1.0f + t1);
+        *d_next = -k * t1 * (1.0f + t0) * inv * inv;
+        *d_this = k * t0 * inv;
     } else {
-        const float q = 1.0f / (1.0f + e1);
-        *d_next = -k * (1.0f + e0) * q * (1.0f - q);
-        *d_this = k * e0 * q;
+        const float keep = k * expf(t0 - t1);
+        *d_next = keep * expm1f(-t1);
+        *d_this = -keep * expm1f(-t0);
     }
+}
+
+// fixed mode: a first-order distance is trusted only where |grad f| does not vanish and the
+// distance is on the volume's scale (|sdf| <= 4; the box diagonal is 2 sqrt 3); elsewhere the
+// quadric is degenerate at that point and the sample is treated as empty.
+constexpr float kMaxSdf = 4.0f;
+constexpr float kMinGrad2 = 1e-30f;
+template <bool kCompat>
+__device__ __forceinline__ float checked_sdf(const float *a, f3 u, float reso) {
+    const float s = quad_sdf(a, u, reso);
+    if (kCompat) return s;
+    const float nx = 2 * a[0] * u.x + a[3], ny = 2 * a[1] * u.y + a[4], nz = 2 * a[2] * u.z + a[5];
+    const float len2 = nx * nx + ny * ny + nz * nz;
+    return (len2 >= kMinGrad2 && fabsf(s) <= kMaxSdf) ? s : __int_as_float(0x7fc00000);
+}
+
+// The render sample's normal and its gradient.  fixed mode: where grad f vanishes the normal
+// is undefined; it is taken as +z and passes no gradient back.
+template <bool kCompat>
+__device__ __forceinline__ f3 sample_normal(const float *a, f3 u) {
+    if (!kCompat) {
+        const float nx = 2 * a[0] * u.x + a[3], ny = 2 * a[1] * u.y + a[4], nz = 2 * a[2] * u.z + a[5];
+        if (!(nx * nx + ny * ny + nz * nz >= kMinGrad2)) return f3{0.0f, 0.0f, 1.0f};
+    }
+    return quad_normal(a, u);
+}
+template <bool kCompat>
+__device__ __forceinline__ void sample_normal_grad(const float *a, f3 u, f3 gn, float *g) {
+    if (!kCompat) {
+        const float nx = 2 * a[0] * u.x + a[3], ny = 2 * a[1] * u.y + a[4], nz = 2 * a[2] * u.z + a[5];
+        if (!(nx * nx + ny * ny + nz * nz >= kMinGrad2)) {
+#pragma unroll
+            for (int t = 0; t < 6; ++t) g[t] = 0.0f;
+            return;
+        }
+    }
+    quad_normal_grad(a, u, gn, g);
 }
 
 // Per-lane state of one render sample of a chunk.
 struct Sample {
     bool valid;      // sample exists and all its cells are inside the grid
     float alpha;
-    float e0, e1;    // exp(-k sdf_i), exp(-k sdf_{i+1})
+    float e0, e1;    // alpha_term of sdf_i and sdf_{i+1}
     f3 rgb, spec, nrm;
     CellPoint c1;    // SDF sample i+1
     CellPoint cr;    // render sample i
@@ -227,7 +276,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     if (live) {
         if (cell_in_grid(s.c1, R)) {
             Store<S>::cell(p.sdf, (uint32_t)s.c1.index, a1);
-            s1 = quad_sdf(a1, s.c1.u, (float)R);
+            s1 = checked_sdf<kCompat>(a1, s.c1.u, (float)R);
         } else {
             ok = false;
         }
@@ -239,7 +288,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
         if (cell_in_grid(c0, R)) {
             float a0[7];
             Store<S>::cell(p.sdf, (uint32_t)c0.index, a0);
-            s0 = quad_sdf(a0, c0.u, (float)R);
+            s0 = checked_sdf<kCompat>(a0, c0.u, (float)R);
         } else {
             ok = false;
         }
@@ -252,7 +301,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     float ar[7];
     if (live && cell_in_grid(s.cr, R)) {
         Store<S>::cell(p.sdf, (uint32_t)s.cr.index, ar);
-        s.nrm = quad_normal(ar, s.cr.u);
+        s.nrm = sample_normal<kCompat>(ar, s.cr.u);
     } else {
         ok = false;
         s.nrm = f3{0.0f, 0.0f, 1.0f};
@@ -262,8 +311,8 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     // is empty; compat keeps the reference's arithmetic, non-finite values included
     if (!kCompat && !(isfinite(s0) && isfinite(s1))) ok = false;
     s.valid = ok;
-    s.e0 = expf(-p.k * s0);
-    s.e1 = expf(-p.k * s1);
+    s.e0 = alpha_term<kCompat>(p.k, s0);
+    s.e1 = alpha_term<kCompat>(p.k, s1);
     s.alpha = ok ? interval_alpha<kCompat>(s.e0, s.e1) : 0.0f;
     // trilinear weights and base vertex (kernel/render.cu:107-111)
     s.wx = (s.cr.u.x + 1.0f) / 2.0f;
@@ -342,7 +391,7 @@ __device__ __forceinline__ void eval_alpha(const Params &p, uint32_t r, f3 o, f3
         if (cell_in_grid(c1, R)) {
             float a1[7];
             Store<S>::cell(p.sdf, (uint32_t)c1.index, a1);
-            s1 = quad_sdf(a1, c1.u, (float)R);
+            s1 = checked_sdf<kCompat>(a1, c1.u, (float)R);
         } else {
             ok = false;
         }
@@ -354,7 +403,7 @@ __device__ __forceinline__ void eval_alpha(const Params &p, uint32_t r, f3 o, f3
         if (cell_in_grid(c0, R)) {
             float a0[7];
             Store<S>::cell(p.sdf, (uint32_t)c0.index, a0);
-            s0 = quad_sdf(a0, c0.u, (float)R);
+            s0 = checked_sdf<kCompat>(a0, c0.u, (float)R);
         } else {
             ok = false;
         }
@@ -367,8 +416,8 @@ __device__ __forceinline__ void eval_alpha(const Params &p, uint32_t r, f3 o, f3
         ok = false;
     if (!kCompat && !(isfinite(s0) && isfinite(s1))) ok = false;
     s.valid = ok;
-    s.e0 = expf(-p.k * s0);
-    s.e1 = expf(-p.k * s1);
+    s.e0 = alpha_term<kCompat>(p.k, s0);
+    s.e1 = alpha_term<kCompat>(p.k, s1);
     s.alpha = ok ? interval_alpha<kCompat>(s.e0, s.e1) : 0.0f;
 }
 
@@ -624,7 +673,7 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                     const f3 gn = shade_any_backward_inplace<kCompat, kDeg>(grgb, s.nrm, d, tile + lane * kRow, s.spec);
                     float ar[7], gr[6];
                     Store<S>::cell(p.sdf, (uint32_t)s.cr.index, ar);
-                    quad_normal_grad(ar, s.cr.u, gn, gr);
+                    sample_normal_grad<kCompat>(ar, s.cr.u, gn, gr);
                     if (s.cr.index == s.c1.index) {
 #pragma unroll
                         for (int t = 0; t < 6; ++t) gq[t] += gr[t];

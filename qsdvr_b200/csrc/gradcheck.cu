@@ -61,14 +61,22 @@ __device__ d3 shade64(d3 n, d3 v, const double *d) {
     return d3{(d[27] * (1.0 - m) + s.x * m) * ao, (d[28] * (1.0 - m) + s.y * m) * ao, (d[29] * (1.0 - m) + s.z * m) * ao};
 }
 
+// SDF sample j and whether fixed mode trusts it (|grad f|^2 >= 1e-30 and |sdf| <= 4, the
+// rule of the fused kernels); an interval with an untrusted end is empty.
 __device__ double sample_sdf(const double *g8, f3 o, f3 dir, uint32_t j, float interval, float vo, uint32_t R,
-                             bool *ok) {
+                             bool *ok, bool *trusted) {
     const CellPoint c = to_cell(march(o, dir, (float)j, interval), vo, R);
     if (!in_grid(c, R)) {
         *ok = false;
+        *trusted = false;
         return 0.0;
     }
-    return sdf64(g8 + 8ull * (uint32_t)c.index, d3{c.u.x, c.u.y, c.u.z}, (double)R);
+    const double *a = g8 + 8ull * (uint32_t)c.index;
+    const d3 u{c.u.x, c.u.y, c.u.z};
+    const double nx = 2 * a[0] * u.x + a[3], ny = 2 * a[1] * u.y + a[4], nz = 2 * a[2] * u.z + a[5];
+    const double s = sdf64(a, u, (double)R);
+    *trusted = nx * nx + ny * ny + nz * nz >= 1e-30 && fabs(s) <= 4.0;
+    return *trusted ? s : 0.0;
 }
 
 __global__ void __launch_bounds__(128) loss64_kernel(const qsdvr_ray_info *__restrict__ rays,
@@ -86,11 +94,12 @@ __global__ void __launch_bounds__(128) loss64_kernel(const qsdvr_ray_info *__res
     bool ok = true;
     d3 C{0.0, 0.0, 0.0};
     double T = 1.0;
-    double e0 = nr ? exp(-k * sample_sdf(g8, o, dv, 0, interval, vo, R, &ok)) : 0.0;
+    bool t0 = false, t1 = false;
+    double e0 = nr ? exp(-k * sample_sdf(g8, o, dv, 0, interval, vo, R, &ok, &t0)) : 0.0;
     for (uint32_t i = 0; i < nr && ok; ++i) {
-        const double e1 = exp(-k * sample_sdf(g8, o, dv, i + 1, interval, vo, R, &ok));
+        const double e1 = exp(-k * sample_sdf(g8, o, dv, i + 1, interval, vo, R, &ok, &t1));
         const double x = (e1 - e0) / (1.0 + e1);
-        const double alpha = x > 0.0 ? x : 0.0;
+        const double alpha = (t0 && t1 && x > 0.0) ? x : 0.0;
         const CellPoint c = to_cell(midpoint(o, dv, i, interval), vo, R);
         if (!in_grid(c, R)) {
             ok = false;
@@ -118,6 +127,7 @@ __global__ void __launch_bounds__(128) loss64_kernel(const qsdvr_ray_info *__res
         C.z += rgb.z * alpha * T;
         T *= (1.0 - alpha);
         e0 = e1;
+        t0 = t1;
     }
     if (!ok) flag_error(QSDVR_DEVERR_INDEX);
     const double ex = C.x - target[3 * r], ey = C.y - target[3 * r + 1], ez = C.z - target[3 * r + 2];

@@ -64,6 +64,8 @@ def parser():
     ap.add_argument("--mode", default="fixed", choices=["fixed", "compat"])
     ap.add_argument("--sh", type=int, default=2, choices=[2, 3])
     ap.add_argument("--proposal", action="store_true", help="train at the proposal network's fine samples")
+    ap.add_argument("--online-proposal", action="store_true",
+                    help="train the grid with the uniform march and the proposal network online beside it")
     ap.add_argument("--proposal-rays", type=int, default=4096, help="rays of the per-step uniform pass")
     ap.add_argument("--proposal-points", type=int, default=65536, help="MLP training points per step")
     ap.add_argument("--proposal-lr", type=float, default=5e-3)
@@ -73,11 +75,12 @@ def parser():
     return ap
 
 
-def run(a, data=None, quiet=False):
+def run(a, data=None, quiet=False, return_state=False):
     """Train per ``a`` (parser() namespace).  ``data``: (rays, origin, dir, target) to reuse
     a built scene.  Returns the summary dict; its "render_ms" is the device time of the
-    render part of the steps (forward + backward, and for --proposal the coarse MLP, the
-    sampler and the online network update), "optimizer_ms" that of the grid Adam steps."""
+    render part of the steps (forward + backward, and with a proposal network the coarse MLP,
+    the sampler and the online network update), "optimizer_ms" that of the grid Adam steps.
+    ``return_state``: also return the trained model and proposal network (or None)."""
     from .proposal import ProposalNet
 
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -95,7 +98,7 @@ def run(a, data=None, quiet=False):
     opt = FusedGridAdam(model.parameters(), lr=a.lr, bf16_copies=copies)
     model.sdfGrid.grad = torch.zeros_like(model.sdfGrid)
     model.renderData.grad = torch.zeros_like(model.renderData)
-    net = ProposalNet(dev, seed=a.seed, lr=a.proposal_lr) if a.proposal else None
+    net = ProposalNet(dev, seed=a.seed, lr=a.proposal_lr) if (a.proposal or a.online_proposal) else None
     loss = torch.zeros(1, dtype=torch.float32, device=dev)
     log = []
 
@@ -128,7 +131,8 @@ def run(a, data=None, quiet=False):
             n = min(a.proposal_rays, a.rays)
             net.online_step(r[:n], o[:n], d[:n], sg, dg, R, a.interval, a.k, a.mode, model.transmittance,
                             points=a.proposal_points)
-            tlist = net.sample(r, o, d, a.interval, a.proposal_mix)
+            if a.proposal:
+                tlist = net.sample(r, o, d, a.interval, a.proposal_mix)
         fused.render_train(tg, r, o, d, sg, dg, R, a.interval, a.k, model.sdfGrid.grad, model.renderData.grad,
                            a.mode, model.transmittance, loss=loss, tlist=tlist)
         e1.record()
@@ -145,7 +149,9 @@ def run(a, data=None, quiet=False):
     opt_ms = sum(e1.elapsed_time(e2) for _, e1, e2 in ev)
     end = evaluate()
     out = {"reso": R, "steps": a.steps, "rays_per_step": a.rays, "lr": a.lr, "storage": a.storage, "mode": a.mode,
-           "sh_degree": a.sh, "k": a.k, "method": "proposal 64 coarse + 32 fine" if net else "uniform march",
+           "sh_degree": a.sh, "k": a.k,
+           "method": "proposal 64 coarse + 32 fine" if a.proposal else
+                     "uniform march" + (" + online proposal network" if net else ""),
            "ms_per_step": round(1e3 * elapsed / a.steps, 3), "train_rays_per_s": round(a.steps * a.rays / elapsed),
            "render_ms": round(render_ms, 3), "optimizer_ms": round(opt_ms, 3),
            "render_rays_per_s": round(a.steps * a.rays / (render_ms / 1e3)),
@@ -157,7 +163,7 @@ def run(a, data=None, quiet=False):
         out["heldout_psnr_end_proposal_render"] = round(psnr(end["proposal"]), 3)
     if not quiet:
         print(json.dumps(out), flush=True)
-    return out
+    return (out, model, net) if return_state else out
 
 
 def main(argv=None):
