@@ -357,11 +357,13 @@ def run_ours(args, cfg, device, ws, rank):
 # ----------------------------------------------------------------------------- proposal path
 
 def proposal_comparison(steps: int):
-    """Training at 256^3 with each method from the same initial model on the same batches:
-    the uniform march (256 samples/ray) and the proposal network (64 coarse MLP points + 32
-    fine samples/ray, trained online).  rays/s is device time of the forward + backward part of
-    the steps (for the proposal: coarse MLP, sampler, online network update and the fused
-    train launch); PSNR is on 65536 held-out rays, judged by the uniform march."""
+    """Training at 256^3 from the same initial model on the same ray pool: the uniform march
+    (256 samples/ray, 65536 rays/step) and the proposal path (64 coarse MLP points + 32 fine
+    samples/ray, network trained online every step; twice the rays per step, which costs
+    about the render time of one plain step; the first 20% of its steps use the uniform march
+    while the network learns).  rays/s is device time of the forward + backward part of the
+    steps (for the proposal: coarse MLP, sampler, online network update and the fused train
+    launch); PSNR is on 65536 held-out rays, judged by the uniform march."""
     from qsdvr_b200 import train
 
     a = train.parser().parse_args([])
@@ -369,21 +371,27 @@ def proposal_comparison(steps: int):
     data = train.build(a.reso, a.views, a.size, 1111.1 * a.size / 800, 4.03, a.interval, a.k, a.seed,
                        torch.device("cuda", torch.cuda.current_device()))
     plain = train.run(a, data, quiet=True)
-    a.proposal = True
+    a.proposal, a.rays, a.proposal_mix, a.proposal_warmup = True, 2 * a.rays, 0.05, steps // 5
     prop = train.run(a, data, quiet=True)
     del data
     torch.cuda.empty_cache()
     return {"method": "64 coarse MLP points + 32 fine samples per ray (tcgen05 MLP, trained online)",
-            "workload": f"R={a.reso}^3 fp32 fixed mode, {a.rays} rays/step, {steps} training steps per method from "
-                        f"the same sphere init, k={a.k}, Adam lr {a.lr}",
+            "workload": f"R={a.reso}^3 fp32 fixed mode, {steps} training steps per method from the same sphere "
+                        f"init, k={a.k}, Adam lr {a.lr}; plain {plain['rays_per_step']} rays/step, proposal "
+                        f"{prop['rays_per_step']} rays/step with {a.proposal_warmup} uniform warm-up steps",
             "train_rays_per_s": prop["render_rays_per_s"], "plain_train_rays_per_s": plain["render_rays_per_s"],
             "speedup": round(prop["render_rays_per_s"] / plain["render_rays_per_s"], 3),
+            "steady_train_rays_per_s": prop["steady_render_rays_per_s"],
+            "steady_speedup": round(prop["steady_render_rays_per_s"] / plain["render_rays_per_s"], 3),
             "render_ms_per_step": round(prop["render_ms"] / steps, 4),
             "plain_render_ms_per_step": round(plain["render_ms"] / steps, 4),
             "optimizer_ms_per_step": round(prop["optimizer_ms"] / steps, 4),
             "psnr_plain": plain["heldout_psnr_end"], "psnr_proposal": prop["heldout_psnr_end"],
             "delta_psnr": round(plain["heldout_psnr_end"] - prop["heldout_psnr_end"], 3),
-            "judge": "held-out rays rendered with the 256-sample uniform march vs ground truth"}
+            "psnr_proposal_render": prop["heldout_psnr_end_proposal_render"],
+            "delta_psnr_method": round(plain["heldout_psnr_end"] - prop["heldout_psnr_end_proposal_render"], 3),
+            "judge": "held-out rays vs ground truth: delta_psnr with both models rendered by the 256-sample "
+                     "uniform march, delta_psnr_method with each model rendered by its own method"}
 
 
 def run_proposal_frames(args, cfg, device):

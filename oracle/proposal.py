@@ -8,7 +8,8 @@ specification the CUDA kernels (qsdvr_b200/csrc/proposal.cu) are checked against
   the layer-1 bias, 4 zeros) -> 64 ReLU -> 64 ReLU -> softplus.  Parameters are the bf16
   copy the kernels read.  The kernels round the encoding and the first hidden layer to bf16
   before the tensor-core GEMMs, and in training the two back-propagated hidden gradients as
-  well; the oracle applies the same roundings (round to nearest even) and does every other
+  well (db2 is summed from the rounded layer-2 gradient, as the GEMM that yields it does);
+  the oracle applies the same roundings (round to nearest even) and does every other
   operation in float64.
 * Loss per point: w (log1p(s) - log1p(t))^2, w = under_weight where s < t, mean over points;
   points with a negative target are ignored (they still count in the mean's denominator).
@@ -96,8 +97,8 @@ def train_gradients(params, points, under_weight: float, round_grads: bool = Tru
     g[OFF_B3] = dy.sum()
     g[OFF_W3:OFF_B3] = f["h2"].T @ dy
     dh2 = np.where(f["z2"] > 0.0, dy[:, None] * w["w3"][None, :], 0.0)
-    g[OFF_B2:OFF_W3] = dh2.sum(0)
     dh2b = rnd(dh2)
+    g[OFF_B2:OFF_W3] = dh2b.sum(0)  # db2 comes out of the bf16 dW2 GEMM (H1's constant feature)
     g[OFF_W2:OFF_B2] = (dh2b.T @ f["h1"]).reshape(-1)
     dh1 = np.where(f["d1"] > 0.0, dh2b @ w["W2"], 0.0)
     dh1b = rnd(dh1)

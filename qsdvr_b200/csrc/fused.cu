@@ -734,17 +734,26 @@ struct Layout {
 };
 
 struct Occupancy {
-    int per_sm = 0;
+    int pass = kTrain;
+    int per_sm = 0, train_per_sm = 0;
     size_t chunk_bytes = 0;
     cudaError_t err = cudaSuccess;
     template <bool C, typename S, bool L, int D>
     void run() {
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<C, S, kTrain, L, D>, kThreads, 0);
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&train_per_sm, render_kernel<C, S, kTrain, L, D>, kThreads, 0);
+        per_sm = train_per_sm;
+        if (err == cudaSuccess && pass == kForward)
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<C, S, kForward, L, D>, kThreads, 0);
+        if (err == cudaSuccess && pass == kBackward)
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<C, S, kBackward, L, D>, kThreads, 0);
         chunk_bytes = chunk_floats<D>() * sizeof(float);
     }
 };
 
-Layout layout_for(const qsdvr_render_args *a) {
+// Persistent grid of a pass: as many one-warp blocks as are resident (each pass has its own
+// register use, so the forward runs more warps per SM than the train kernel); the train
+// pass's stash slots are sized by its own grid.
+Layout layout_for(const qsdvr_render_args *a, int pass = kTrain) {
     Layout L{QSDVR_OK, 0, kCounterBytes, 0};
     int dev = 0, sms = 0;
     if (check_cuda(cudaGetDevice(&dev), "render: cudaGetDevice") != QSDVR_OK ||
@@ -753,15 +762,18 @@ Layout layout_for(const qsdvr_render_args *a) {
         return L;
     }
     Occupancy occ;
+    occ.pass = pass;
     dispatch(a, occ);
     if (check_cuda(occ.err, "render: occupancy") != QSDVR_OK) {
         L.error = QSDVR_ERR_CUDA;
         return L;
     }
     L.blocks = (unsigned)(sms * (occ.per_sm > 0 ? occ.per_sm : 1));
-    L.train_bytes = kCounterBytes + (size_t)L.blocks * kWarpsPerBlock * kSlotChunks * occ.chunk_bytes;
+    const size_t train_blocks = (size_t)sms * (occ.train_per_sm > 0 ? occ.train_per_sm : 1);
+    L.train_bytes = kCounterBytes + train_blocks * kWarpsPerBlock * kSlotChunks * occ.chunk_bytes;
     return L;
 }
+
 
 template <int kPass>
 struct Launcher {
@@ -801,7 +813,7 @@ int launch(const qsdvr_render_args *a, cudaStream_t stream) {
     p.sample_capacity = a->sample_capacity;
     unsigned blocks = grid_for(a->ray_count, kWarpsPerBlock);
     if (a->workspace) {
-        const Layout L = layout_for(a);
+        const Layout L = layout_for(a, kPass);
         if (L.error != QSDVR_OK) return L.error;
         if (a->workspace_bytes < (kPass == kTrain ? L.train_bytes : L.counter_bytes))
             return set_error(QSDVR_ERR_WORKSPACE, "render: workspace %llu < %zu bytes",

@@ -14,6 +14,8 @@
 //   [6144, 6208) b2[64]   [6208, 6272) w3[64]   [6272] b3   (padded to 6280)
 // Encoding of p in [-1,1]^3: f0..2 = p, f(3 + 6l + 2c) = sin(pi 2^l p_c), f(4 + 6l + 2c) =
 // cos(pi 2^l p_c) for l = 0..3, f27 = 1, f28..31 = 0.  Density bound = softplus(w3 . h2 + b3).
+// b2 rides in the layer-2 GEMM: the staged H1 has a constant feature 64 = 1 and the staged
+// W2 a column 64 = b2 (K = 80), so in training the dW2 GEMM also yields db2 (its column 64).
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -35,9 +37,12 @@ constexpr uint32_t kTrainCols = 256;   // of a training CTA: forward 0..63, dW2 
 
 // shared-memory operand layouts (bytes): element (row, feature) of an activation buffer with
 // point-group stride SP sits at (row/8)*SP + (f/8)*128 + (row%8)*16 + (f%8)*2
-constexpr uint32_t kSpX = 512, kSpH = 1024, kSpG = 2048;  // X (32 f), H1 (64 f), grads (64 f + 64 zero)
+constexpr uint32_t kSpX = 512, kSpH = 1280, kSpG = 2048;  // X (32 f), H1 (64 f + bias 1 + 15 zero),
+                                                           // grads (64 f + 64 zero)
+constexpr uint32_t kSoW1 = 512, kSoW2 = 1280;              // W1 (32 inputs), W2 (64 inputs + b2 + 15 zero)
+constexpr uint32_t kK2 = 80;                               // layer-2 K with the bias feature
 constexpr uint32_t kBytesX = 16 * kSpX, kBytesH = 16 * kSpH, kBytesG = 16 * kSpG;
-constexpr uint32_t kBytesW1 = 8 * 512, kBytesW2 = 8 * 1024;
+constexpr uint32_t kBytesW1 = 8 * kSoW1, kBytesW2 = 8 * kSoW2;
 
 __device__ __forceinline__ uint32_t act_off(uint32_t row, uint32_t f, uint32_t sp) {
     return (row >> 3) * sp + (f >> 3) * 128 + (row & 7) * 16 + (f & 7) * 2;
@@ -50,6 +55,23 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
 
 __device__ __forceinline__ float bf16f(const __nv_bfloat16 *p, int i) { return __bfloat162float(p[i]); }
 
+// Two floats -> bf16x2 with ReLU applied, one instruction (cvt.rn.relu.bf16x2.f32).
+__device__ __forceinline__ uint32_t pack_relu_bf16(float a, float b) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+    return r;
+}
+
+// Write 8 consecutive features [8g, 8g+8) of one row, ReLU applied, as one 16-byte store.
+__device__ __forceinline__ void store_relu_row8(uint8_t *buf, uint32_t row, uint32_t g, uint32_t sp, const float *v) {
+    uint4 q;
+    q.x = pack_relu_bf16(v[0], v[1]);
+    q.y = pack_relu_bf16(v[2], v[3]);
+    q.z = pack_relu_bf16(v[4], v[5]);
+    q.w = pack_relu_bf16(v[6], v[7]);
+    *reinterpret_cast<uint4 *>(buf + act_off(row, 8 * g, sp)) = q;
+}
+
 // Write 8 consecutive features [8g, 8g+8) of one row as one 16-byte store.
 __device__ __forceinline__ void store_row8(uint8_t *buf, uint32_t row, uint32_t g, uint32_t sp, const float *v) {
     uint4 q;
@@ -60,18 +82,18 @@ __device__ __forceinline__ void store_row8(uint8_t *buf, uint32_t row, uint32_t 
     *reinterpret_cast<uint4 *>(buf + act_off(row, 8 * g, sp)) = q;
 }
 
-// The octaves 2^l (l = 1..3) come from the first by the double-angle identities
-// sin 2a = 2 sin a cos a, cos 2a = 1 - 2 sin^2 a: three sincospif per point instead of twelve;
-// the recurrence's error (~1e-6) is far below the bf16 rounding that follows.
+// The base octave uses the hardware sine/cosine (absolute error about 2^-21 on [-pi, pi]); the
+// octaves 2^l (l = 1..3) follow by the double-angle identities sin 2a = 2 sin a cos a,
+// cos 2a = 1 - 2 sin^2 a.  Both errors (~1e-6) are far below the bf16 rounding that follows.
 __device__ __forceinline__ void encode(f3 p, float *f) {
+    constexpr float kPi = 3.14159265358979f;
     f[0] = p.x;
     f[1] = p.y;
     f[2] = p.z;
     const float c[3] = {p.x, p.y, p.z};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        float sn, cs;
-        sincospif(c[k], &sn, &cs);
+        float sn = __sinf(kPi * c[k]), cs = __cosf(kPi * c[k]);
 #pragma unroll
         for (int l = 0; l < 4; ++l) {
             f[3 + 6 * l + 2 * k] = sn;
@@ -85,21 +107,28 @@ __device__ __forceinline__ void encode(f3 p, float *f) {
     f[28] = f[29] = f[30] = f[31] = 0.0f;
 }
 
-__device__ __forceinline__ float softplus(float y) { return y > 20.0f ? y : log1pf(expf(y)); }
-__device__ __forceinline__ float sigmoid(float y) { return 1.0f / (1.0f + expf(-y)); }
+__device__ __forceinline__ float softplus(float y) { return y > 20.0f ? y : __logf(1.0f + __expf(y)); }
+__device__ __forceinline__ float sigmoid(float y) { return 1.0f / (1.0f + __expf(-y)); }
 
 // Stage W1 / W2 (bf16) in their canonical K-major layouts: element (o, i) at
-// (o/8)*SO + (i/8)*128 + (o%8)*16 + (i%8)*2 with SO = 512 (W1) or 1024 (W2).
-__device__ void stage_weights(const __nv_bfloat16 *w, uint8_t *w1s, uint8_t *w2s) {
+// (o/8)*SO + (i/8)*128 + (o%8)*16 + (i%8)*2 with SO = kSoW1 (W1) or kSoW2 (W2; its column 64
+// is b2, columns 65..79 zero).  Also the constant features 64..79 (1, 0, ..) of H1 row t.
+__device__ void stage_weights(const __nv_bfloat16 *w, uint8_t *w1s, uint8_t *w2s, uint8_t *hs) {
     for (int idx = threadIdx.x; idx < 64 * 4; idx += blockDim.x) {  // W1: 64 rows x 4 groups
         const int o = idx >> 2, g = idx & 3;
-        *reinterpret_cast<uint4 *>(w1s + act_off(o, 8 * g, 512)) = *reinterpret_cast<const uint4 *>(w + o * 32 + 8 * g);
+        *reinterpret_cast<uint4 *>(w1s + act_off(o, 8 * g, kSoW1)) =
+            *reinterpret_cast<const uint4 *>(w + o * 32 + 8 * g);
     }
-    for (int idx = threadIdx.x; idx < 64 * 8; idx += blockDim.x) {  // W2: 64 rows x 8 groups
-        const int o = idx >> 3, g = idx & 7;
-        *reinterpret_cast<uint4 *>(w2s + act_off(o, 8 * g, 1024)) =
-            *reinterpret_cast<const uint4 *>(w + kOffW2 + o * 64 + 8 * g);
+    for (int idx = threadIdx.x; idx < 64 * 10; idx += blockDim.x) {  // W2: 64 rows x 10 groups
+        const int o = idx / 10, g = idx % 10;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (g < 8) v = *reinterpret_cast<const uint4 *>(w + kOffW2 + o * 64 + 8 * g);
+        else if (g == 8) v.x = (uint32_t)__bfloat16_as_ushort(w[kOffB2 + o]);  // (b2[o], 0)
+        *reinterpret_cast<uint4 *>(w2s + act_off(o, 8 * g, kSoW2)) = v;
     }
+    const uint32_t one = (uint32_t)__bfloat16_as_ushort(__float2bfloat16(1.0f));
+    *reinterpret_cast<uint4 *>(hs + act_off(threadIdx.x, 64, kSpH)) = make_uint4(one, 0, 0, 0);
+    *reinterpret_cast<uint4 *>(hs + act_off(threadIdx.x, 72, kSpH)) = make_uint4(0, 0, 0, 0);
 }
 
 struct Sync {
@@ -128,17 +157,18 @@ __device__ __forceinline__ void handoff() {
 }
 
 // Forward of one tile: X (staged) -> H1 (staged, returns the relu mask) -> z2 = W2 h1 + b2
-// (this thread's row, in registers).  Both layers accumulate in the same 64 TMEM columns at
-// d1: every thread has read layer 1's result before the barrier that precedes layer 2.
+// (this thread's row, in registers; b2 through H1's constant feature).  Both layers
+// accumulate in the same 64 TMEM columns at d1: every thread has read layer 1's result before
+// the barrier that precedes layer 2.
 __device__ __forceinline__ uint64_t forward_tile(uint8_t *xs, uint8_t *hs, uint8_t *w1s, uint8_t *w2s, uint32_t d1,
-                                                 Sync &sync, const float *b2, float *z2) {
+                                                 Sync &sync, float *z2) {
     const uint32_t t = threadIdx.x, warp = t >> 5;
     constexpr uint32_t i1 = tc::idesc_bf16(128, 64, false, false);
     handoff();
     if (t == 0) {
         for (int s = 0; s < 2; ++s)
             tc::mma_bf16(d1, tc::smem_desc(tc::smem_addr(xs) + 256 * s, 128, kSpX),
-                         tc::smem_desc(tc::smem_addr(w1s) + 256 * s, 128, 512), i1, s > 0);
+                         tc::smem_desc(tc::smem_addr(w1s) + 256 * s, 128, kSoW1), i1, s > 0);
     }
     sync.complete();
     uint64_t mask = 0;
@@ -146,30 +176,26 @@ __device__ __forceinline__ uint64_t forward_tile(uint8_t *xs, uint8_t *hs, uint8
         float v[64];
         tc::tmem_ld64(tc::tmem_at(d1, 32 * warp, 0), v);
 #pragma unroll
-        for (int q = 0; q < 64; ++q) {
-            if (v[q] > 0.0f) mask |= 1ull << q;
-            v[q] = fmaxf(v[q], 0.0f);
-        }
+        for (int q = 0; q < 64; ++q)
+            if (v[q] > 0.0f) mask |= 1ull << q;  // only the training kernel uses the mask
 #pragma unroll
-        for (int g = 0; g < 8; ++g) store_row8(hs, t, g, kSpH, v + 8 * g);
+        for (int g = 0; g < 8; ++g) store_relu_row8(hs, t, g, kSpH, v + 8 * g);
     }
     handoff();
     if (t == 0) {
-        for (int s = 0; s < 4; ++s)
+        for (int s = 0; s < (int)kK2 / 16; ++s)
             tc::mma_bf16(d1, tc::smem_desc(tc::smem_addr(hs) + 256 * s, 128, kSpH),
-                         tc::smem_desc(tc::smem_addr(w2s) + 256 * s, 128, 1024), i1, s > 0);
+                         tc::smem_desc(tc::smem_addr(w2s) + 256 * s, 128, kSoW2), i1, s > 0);
     }
     sync.complete();
     tc::tmem_ld64(tc::tmem_at(d1, 32 * warp, 0), z2);
-#pragma unroll
-    for (int q = 0; q < 64; ++q) z2[q] += b2[q];
     return mask;
 }
 
 // ---- training -------------------------------------------------------------------------------
 
 struct TrainSmem {
-    float b2[64], w3[64], db2[64], dw3[64], db3, loss;
+    float w3[64], dw3[64], db3, loss;
     uint64_t mbar;
     uint32_t tmem;
 };
@@ -192,11 +218,9 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
     // zero the gradient operand buffers (their upper 64 feature columns stay zero: rows
     // 64..127 of the padded M = 128 weight-gradient GEMMs)
     for (uint32_t i = t; i < 2 * kBytesG / 16; i += 128) reinterpret_cast<uint4 *>(g2)[i] = make_uint4(0, 0, 0, 0);
-    stage_weights(w, w1s, w2s);
+    stage_weights(w, w1s, w2s, hs);
     if (t < 64) {
-        S.b2[t] = bf16f(w, kOffB2 + t);
         S.w3[t] = bf16f(w, kOffW3 + t);
-        S.db2[t] = 0.0f;
         S.dw3[t] = 0.0f;
     }
     if (t == 0) {
@@ -211,7 +235,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
     const uint32_t tmem = S.tmem;
     const float b3 = bf16f(w, kOffB3);
     Sync sync{&S.mbar, 0u, true};
-    constexpr uint32_t kD1 = 0, kDW2 = 128, kDW1 = 192;
+    constexpr uint32_t kD1 = 0, kDW2 = 128, kDW1 = 224;  // dW2: 80 columns (64 + db2 + pad), dW1: 32
     const uint32_t tiles = (P + kTile - 1) / kTile;
     bool first = true;
     float my_db3 = 0.0f, my_loss = 0.0f;
@@ -227,7 +251,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
             for (int q = 0; q < 4; ++q) store_row8(xs, t, q, kSpX, f + 8 * q);
         }
         float z2[kH];
-        const uint64_t mask1 = forward_tile(xs, hs, w1s, w2s, tmem + kD1, sync, S.b2, z2);
+        const uint64_t mask1 = forward_tile(xs, hs, w1s, w2s, tmem + kD1, sync, z2);
         if (!sync.ok) break;
         // head, loss and its gradient
         float y = b3;
@@ -247,17 +271,11 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
         for (int o = 0; o < kH; ++o) {
             const float h2 = fmaxf(z2[o], 0.0f);
             dh2[o] = z2[o] > 0.0f ? dy * S.w3[o] : 0.0f;
-            // warp-reduce this output's dw3 and db2 partials, one shared add per warp
-            float a = dy * h2, b = dh2[o];
+            // warp-reduce this output's dw3 partial, one shared add per warp
+            float a = dy * h2;
 #pragma unroll
-            for (int off = 16; off; off >>= 1) {
-                a += __shfl_xor_sync(kFull, a, off);
-                b += __shfl_xor_sync(kFull, b, off);
-            }
-            if (lane == 0) {
-                atomicAdd(&S.dw3[o], a);
-                atomicAdd(&S.db2[o], b);
-            }
+            for (int off = 16; off; off >>= 1) a += __shfl_xor_sync(kFull, a, off);
+            if (lane == 0) atomicAdd(&S.dw3[o], a);
         }
 #pragma unroll
         for (int q = 0; q < 8; ++q) store_row8(g2, t, q, kSpG, dh2 + 8 * q);
@@ -267,9 +285,10 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
             constexpr uint32_t i_dh1 = tc::idesc_bf16(128, 64, false, true);
             for (int s4 = 0; s4 < 4; ++s4)
                 tc::mma_bf16(tmem + kD1, tc::smem_desc(tc::smem_addr(g2) + 256 * s4, 128, kSpG),
-                             tc::smem_desc(tc::smem_addr(w2s) + 2 * 1024 * s4, 1024, 128), i_dh1, s4 > 0);
-            // dW2 += dH2^T H1  (A: dH2 MN-major, M = o padded to 128;  B: H1 MN-major, N = i;  K = points)
-            constexpr uint32_t i_dw2 = tc::idesc_bf16(128, 64, true, true);
+                             tc::smem_desc(tc::smem_addr(w2s) + 2 * kSoW2 * s4, kSoW2, 128), i_dh1, s4 > 0);
+            // dW2 += dH2^T H1 (A: dH2 MN-major, M = o padded to 128;  B: H1 MN-major, N = i
+            // including the constant feature 64, whose column is db2;  K = points)
+            constexpr uint32_t i_dw2 = tc::idesc_bf16(128, kK2, true, true);
             for (int s8 = 0; s8 < 8; ++s8)
                 tc::mma_bf16(tmem + kDW2, tc::smem_desc(tc::smem_addr(g2) + 2 * kSpG * s8, kSpG, 128),
                              tc::smem_desc(tc::smem_addr(hs) + 2 * kSpH * s8, kSpH, 128), i_dw2, !(first && s8 == 0));
@@ -307,6 +326,11 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
 #pragma unroll
                 for (int q = 0; q < 16; ++q) atomicAdd(&grad[kOffW2 + o * 64 + 16 * j + q], v[q]);
             }
+            {
+                float v[16];
+                tc::tmem_ld16(tc::tmem_at(tmem, 32 * warp, kDW2 + 64), v);
+                atomicAdd(&grad[kOffB2 + o], v[0]);
+            }
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
                 float v[16];
@@ -327,10 +351,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
     tc::fence_before_sync();
     __syncthreads();
     if (sync.ok && !first) {
-        if (t < 64) {
-            atomicAdd(&grad[kOffB2 + t], S.db2[t]);
-            atomicAdd(&grad[kOffW3 + t], S.dw3[t]);
-        }
+        if (t < 64) atomicAdd(&grad[kOffW3 + t], S.dw3[t]);
         if (t == 0) {
             atomicAdd(&grad[kOffB3], S.db3);
             atomicAdd(loss_out, S.loss / (float)P);
@@ -342,7 +363,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
 // ---- inference --------------------------------------------------------------------------
 
 struct InferSmem {
-    float b2[64], w3[64];
+    float w3[64];
     uint64_t mbar;
     uint32_t tmem;
 };
@@ -381,11 +402,8 @@ __global__ void __launch_bounds__(128, 5) mlp_infer_kernel(const float4 *__restr
     uint8_t *w2s = w1s + kBytesW1;
     InferSmem &S = *reinterpret_cast<InferSmem *>(w2s + kBytesW2);
     const uint32_t t = threadIdx.x, warp = t >> 5;
-    stage_weights(w, w1s, w2s);
-    if (t < 64) {
-        S.b2[t] = bf16f(w, kOffB2 + t);
-        S.w3[t] = bf16f(w, kOffW3 + t);
-    }
+    stage_weights(w, w1s, w2s, hs);
+    if (t < 64) S.w3[t] = bf16f(w, kOffW3 + t);
     if (t == 0) tc::mbar_init(&S.mbar, 1);
     if (warp == 0) tc::tmem_alloc(&S.tmem, kInferCols);
     tc::fence_before_sync();
@@ -423,7 +441,7 @@ __global__ void __launch_bounds__(128, 5) mlp_infer_kernel(const float4 *__restr
         if (next < tiles && gn < total) p = infer_input(pts, rays, origin, dir, interval, gn);
         live = next < tiles && gn < total && (!rays || rays[gn >> 6].sdf_count > 1);
         float z2[kH];
-        forward_tile(xs, hs, w1s, w2s, tmem, sync, S.b2, z2);
+        forward_tile(xs, hs, w1s, w2s, tmem, sync, z2);
         float y = b3;
 #pragma unroll
         for (int o = 0; o < kH; ++o) y += S.w3[o] * fmaxf(z2[o], 0.0f);

@@ -10,8 +10,9 @@ every view; the model starts from a sphere SDF and constant appearance (models/r
 their gradients and Adam state is O(rays).
 
 ``--proposal`` trains the grid at the proposal network's 32 fine samples per ray (64 coarse
-MLP evaluations place them) instead of the uniform march.  The network is trained online
-every step on the per-sample alphas of a uniform-march forward over part of the batch.
+MLP evaluations place them) instead of the uniform march (after ``--proposal-warmup`` steps
+with it).  The network is trained online every step on the per-sample alphas of a
+uniform-march forward over part of the batch.
 Held-out PSNR is always measured with the uniform march (the judge).
 """
 from __future__ import annotations
@@ -70,6 +71,8 @@ def parser():
     ap.add_argument("--proposal-points", type=int, default=65536, help="MLP training points per step")
     ap.add_argument("--proposal-lr", type=float, default=5e-3)
     ap.add_argument("--proposal-mix", type=float, default=0.25, help="uniform share of the fine-sample pdf")
+    ap.add_argument("--proposal-warmup", type=int, default=0,
+                    help="steps trained with the uniform march (network trained online) before the proposal")
     ap.add_argument("--log-every", type=int, default=100)
     ap.add_argument("--seed", type=int, default=0)
     return ap
@@ -131,7 +134,7 @@ def run(a, data=None, quiet=False, return_state=False):
             n = min(a.proposal_rays, a.rays)
             net.online_step(r[:n], o[:n], d[:n], sg, dg, R, a.interval, a.k, a.mode, model.transmittance,
                             points=a.proposal_points)
-            if a.proposal:
+            if a.proposal and step > a.proposal_warmup:
                 tlist = net.sample(r, o, d, a.interval, a.proposal_mix)
         fused.render_train(tg, r, o, d, sg, dg, R, a.interval, a.k, model.sdfGrid.grad, model.renderData.grad,
                            a.mode, model.transmittance, loss=loss, tlist=tlist)
@@ -147,6 +150,8 @@ def run(a, data=None, quiet=False, return_state=False):
     elapsed = time.perf_counter() - t0
     render_ms = sum(e0.elapsed_time(e1) for e0, e1, _ in ev)
     opt_ms = sum(e1.elapsed_time(e2) for _, e1, e2 in ev)
+    warm = a.proposal_warmup if a.proposal else 0
+    steady = [e0.elapsed_time(e1) for e0, e1, _ in ev[warm:]]
     end = evaluate()
     out = {"reso": R, "steps": a.steps, "rays_per_step": a.rays, "lr": a.lr, "storage": a.storage, "mode": a.mode,
            "sh_degree": a.sh, "k": a.k,
@@ -155,6 +160,7 @@ def run(a, data=None, quiet=False, return_state=False):
            "ms_per_step": round(1e3 * elapsed / a.steps, 3), "train_rays_per_s": round(a.steps * a.rays / elapsed),
            "render_ms": round(render_ms, 3), "optimizer_ms": round(opt_ms, 3),
            "render_rays_per_s": round(a.steps * a.rays / (render_ms / 1e3)),
+           "steady_render_rays_per_s": round(len(steady) * a.rays / (sum(steady) / 1e3)) if steady else None,
            "heldout_psnr_start": round(psnr(start["uniform"]), 3), "heldout_psnr_end": round(psnr(end["uniform"]), 3),
            "peak_memory_gb": round(torch.cuda.max_memory_allocated(dev) / 1e9, 3),
            "model_and_state_gb": round((torch.cuda.max_memory_allocated(dev) - base_mem) / 1e9, 3),
