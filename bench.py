@@ -49,6 +49,10 @@ WORKLOADS = {
                     storage="f32", sh=3),
     # learned proposal form: full-frame renders of a trained 384^3 BF16 SH3 model, 64 coarse MLP
     # points + 32 fine samples per ray against the 512-sample uniform march
+    # the proposal network's kernels at the training batch: coarse MLP inference (64 points per
+    # ray) against the tensor roofline, beside the sampler, MLP training and the renders
+    "mlp256": dict(R=256, rays=65536, views=20, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
+                   storage="f32", online_steps=200),
     "proposal384": dict(R=384, rays=65536, views=200, size=800, focal=1111.1, radius=4.03, interval=4.0 / 512,
                         storage="bf16", sh=3, train_steps=200, heldout=4),
 }
@@ -216,8 +220,9 @@ def samples_of(batch):
 
 # ----------------------------------------------------------------------------- timing
 
-def time_device(step, steps, warmup, stream, clock=None):
-    """Warm-up, then K steps between two events; also returns per-step kernel events."""
+def time_device(step, steps, warmup, stream, clock=None, on_start=None):
+    """Warm-up, then K steps between two events; also returns per-step kernel events.
+    ``on_start(start_event)`` lets other streams of the step wait for the region's start."""
     for i in range(warmup):
         step(i, None)
     torch.cuda.synchronize()
@@ -227,6 +232,8 @@ def time_device(step, steps, warmup, stream, clock=None):
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push("timed")
     start.record(stream)
+    if on_start is not None:
+        on_start(start)
     for i in range(steps):
         step(i, ev[i])
     stop.record(stream)
@@ -282,29 +289,41 @@ def run_ours(args, cfg, device, ws, rank):
     host = []
     for b in batches:
         host.append({k: v.cpu().pin_memory() for k, v in b.items()})
-    dev_in = {k: torch.empty_like(v) for k, v in batches[0].items()}
+    # two device input buffers: step i's batch is copied on a copy stream while step i-1's
+    # kernel runs (the copy waits until step i-2 has released the buffer)
+    dev_in = [{k: torch.empty_like(v) for k, v in batches[0].items()} for _ in range(2)]
+    copy_stream = torch.cuda.Stream(device)
+    copied = [torch.cuda.Event() for _ in range(2)]
+    released = [torch.cuda.Event() for _ in range(2)]
+    for e in released:
+        e.record(stream)
     loss_host = torch.zeros(1, dtype=torch.float32).pin_memory()
     h2d = sum(v.numel() * v.element_size() for v in host[0].values())
 
     def e2e_step(i, ev):
-        hb = host[i % len(host)]
-        for k, v in hb.items():
-            dev_in[k].copy_(v, non_blocking=True)
+        hb, buf = host[i % len(host)], dev_in[i % 2]
+        with torch.cuda.stream(copy_stream):
+            copy_stream.wait_event(released[i % 2])
+            for k, v in hb.items():
+                buf[k].copy_(v, non_blocking=True)
+            copied[i % 2].record(copy_stream)
         sg.zero_()
         dg.zero_()
         loss.zero_()
+        stream.wait_event(copied[i % 2])
         if ev is not None:
             ev[0].record(stream)
-        fused.render_train(dev_in["target"], dev_in["rays"], dev_in["origin"], dev_in["dir"], sdf_k, data_k, R,
+        fused.render_train(buf["target"], buf["rays"], buf["origin"], buf["dir"], sdf_k, data_k, R,
                            cfg["interval"], K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color)
         if ev is not None:
             ev[1].record(stream)
+        released[i % 2].record(stream)
         loss_host.copy_(loss, non_blocking=True)
 
     if ws > 1:
         torch.distributed.barrier()
     t0 = time.perf_counter()
-    e2e_ms, _ = time_device(e2e_step, args.steps, args.warmup, stream)
+    e2e_ms, _ = time_device(e2e_step, args.steps, args.warmup, stream, on_start=copy_stream.wait_event)
     wall_e2e = time.perf_counter() - t0
     # ---- aggregate over ranks (max time)
     times = torch.tensor([total_ms, e2e_ms, sum(kern_ms) / len(kern_ms)], dtype=torch.float64, device=device)
@@ -392,6 +411,92 @@ def proposal_comparison(steps: int):
             "delta_psnr_method": round(plain["heldout_psnr_end"] - prop["heldout_psnr_end_proposal_render"], 3),
             "judge": "held-out rays vs ground truth: delta_psnr with both models rendered by the 256-sample "
                      "uniform march, delta_psnr_method with each model rendered by its own method"}
+
+
+# algorithmic FLOPs of the 32 -> 64 -> 64 -> 1 network per point (padding of the tensor-core
+# tiles not counted): layer 1 and 2 GEMMs, b2, the head; training adds dH1, dW2, dW1 and the
+# head / bias gradients
+MLP_FLOPS_PER_POINT = 2 * 32 * 64 + 2 * 64 * 64 + 3 * 64
+MLP_TRAIN_FLOPS_PER_POINT = MLP_FLOPS_PER_POINT + 2 * 64 * 64 + 2 * 64 * 64 + 2 * 32 * 64 + 4 * 64
+
+
+def run_mlp_kernels(args, cfg, device):
+    """Coarse MLP inference over a 65536-ray batch (4.2 M points) timed over K launches, with
+    the tensor roofline; the other proposal kernels and both render modes timed beside it."""
+    from qsdvr_b200 import fused, proposal, scenes, train
+
+    R, interval, k = cfg["R"], cfg["interval"], 5.0
+    rays, origin, direction, target = train.build(R, cfg["views"], cfg["size"], cfg["focal"], cfg["radius"],
+                                                  interval, k, 0, device)
+    sdf = fused.pad_grid7(scenes.procedural_grid(R, seed=0, device=device).reshape(-1, 7))
+    data = scenes.appearance(R, seed=0, device=device, procedural=True)
+    gen = torch.Generator(device=device).manual_seed(0)
+    idx = torch.randint(0, rays.shape[0], (cfg["rays"],), generator=gen, device=device)
+    r, o, d, tg = (t[idx].contiguous() for t in (rays, origin, direction, target))
+    net = proposal.ProposalNet(device)
+    for _ in range(cfg["online_steps"]):
+        net.online_step(r[:4096], o[:4096], d[:4096], sdf, data, R, interval, k)
+    stream = torch.cuda.current_stream(device)
+
+    def timed(fn):
+        def step(i, ev):
+            if ev is not None:
+                ev[0].record(stream)
+            fn()
+            if ev is not None:
+                ev[1].record(stream)
+        return time_device(step, args.steps, args.warmup, stream)[0] / args.steps
+
+    with ClockSampler(device.index) as clk:
+        time.sleep(0.3)
+        infer_ms = timed(lambda: net.coarse_density(r, o, d, interval))
+    coarse = net.coarse_density(r, o, d, interval)
+    tl = proposal.sample_fine(r, interval, coarse)
+    pts = torch.rand((cfg["rays"], 4), generator=gen, device=device)
+    sg, dg = torch.zeros_like(sdf), torch.zeros_like(data)
+    side = {
+        "sample_ms": timed(lambda: proposal.sample_fine(r, interval, coarse)),
+        "mlp_train_65536_points_ms": timed(lambda: net.gradients(pts)),
+        "online_step_4096_rays_ms": timed(lambda: net.online_step(r[:4096], o[:4096], d[:4096], sdf, data, R,
+                                                                  interval, k)),
+        "list_train_ms": timed(lambda: fused.render_train(tg, r, o, d, sdf, data, R, interval, k, sg, dg, "fixed",
+                                                          tlist=tl)),
+        "uniform_train_ms": timed(lambda: fused.render_train(tg, r, o, d, sdf, data, R, interval, k, sg, dg,
+                                                             "fixed")),
+        "list_forward_ms": timed(lambda: fused.render_forward(r, o, d, sdf, data, R, interval, k, "fixed",
+                                                              tlist=tl)),
+        "uniform_forward_ms": timed(lambda: fused.render_forward(r, o, d, sdf, data, R, interval, k, "fixed")),
+    }
+    side["mlp_train_tflops"] = round(cfg["rays"] * MLP_TRAIN_FLOPS_PER_POINT / (side["mlp_train_65536_points_ms"]
+                                                                               * 1e-3) / 1e12, 1)
+    side = {kk: (round(v, 4) if isinstance(v, float) else v) for kk, v in side.items()}
+    hit = int((r[:, 0] >= 2).sum())
+    points = cfg["rays"] * 64
+    tflops = points * MLP_FLOPS_PER_POINT / (infer_ms * 1e-3) / 1e12
+    peak = measured_peak_tensor()
+    return {
+        "metric": "proposal MLP coarse-density inference points/s (64 points per ray)",
+        "value": round(points / (infer_ms * 1e-3), 1), "unit": "points/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(infer_ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 (f32 accumulation)", "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": f"mlp256: 32-d encoding -> 64 -> 64 -> 1 on {cfg['rays']} rays of the {R}^3 scene "
+                               f"({hit} with samples), network trained online for {cfg['online_steps']} steps",
+                   "global_batch": points, "l2": "weights in shared memory; inputs 1.6 MB, no flush",
+                   "parallelism": "replicas x1"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "tensor", "achieved": round(tflops, 1), "peak": peak[0], "unit": "TFLOP/s",
+                     "frac": round(tflops / peak[0], 4), "traffic": None, "kernel": "mlp_infer_kernel",
+                     "flops_per_point": MLP_FLOPS_PER_POINT, "peak_kind": peak[1]},
+        "kernels": side, "clocks": clk.summary(),
+    }
+
+
+def measured_peak_tensor():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured (burst)"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
 
 
 def run_proposal_frames(args, cfg, device):
@@ -589,10 +694,11 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=device)
     try:
-        if args.workload == "proposal384":
+        if args.workload in ("proposal384", "mlp256"):
             if ws > 1:
-                raise SystemExit("proposal384 is a single-GPU workload")
-            print(json.dumps(run_proposal_frames(args, cfg, device)))
+                raise SystemExit(f"{args.workload} is a single-GPU workload")
+            fn = run_proposal_frames if args.workload == "proposal384" else run_mlp_kernels
+            print(json.dumps(fn(args, cfg, device)))
             return
         out = run_ours(args, cfg, device, ws, rank)
         if rank == 0:
