@@ -227,6 +227,11 @@ typedef struct qsdvr_render_args {
     float grad_scale;         /* train: dL/dcolor = grad_scale * (color - target) */
     void *workspace;          /* optional, 256-byte aligned: enables the persistent grid with     */
     uint64_t workspace_bytes; /* dynamic ray scheduling and, in train, the per-warp row stash    */
+    const float *sdf_layers;  /* optional, replaces sdf_grid: separable SDF tables [3 reso + 1][4]
+                                 from qsdvr_separable_sdf_tables (fp32 whatever the storage)      */
+    float *sdf_layers_grad;   /* train / backward with sdf_layers: its gradient, same layout,
+                                 zeroed by the caller; qsdvr_separable_sdf_grad turns it into the
+                                 layer and offset gradients                                       */
     const float *tlist;       /* optional [ray_count][33]: SDF sample positions t (from origin) of
                                  each ray, replacing the uniform march (32 render samples at the
                                  interval midpoints); rays with sdf_count < 2 stay empty          */
@@ -234,6 +239,18 @@ typedef struct qsdvr_render_args {
                                  rays[r].render_offset + i (forward and train)                   */
     uint64_t sample_capacity; /* length of sample_alpha */
 } qsdvr_render_args;
+
+/* Separable SDF for the fused renderer (the RenderGrid model's parametrisation,
+ * models/render.py:172-207, without materialising [R^3][7]; LayerToGridForward,
+ * kernel/surface.cu:148-229, computes the same cells): per-axis recurrence tables
+ * [3 reso + 1][4] = (a0, a3, a6, 0) per axis index, then (offset[3], 0, 0, 0). */
+int qsdvr_separable_sdf_tables(const float *x_layer, const float *y_layer, const float *z_layer,
+                               const float *offset, uint32_t reso, float *tables, cudaStream_t stream);
+
+/* Layer gradients from the table gradient the fused renderer accumulated (the reverse
+ * recurrences of LayerToGridBackward, kernel/surface.cu:301-334); table_grad is consumed. */
+int qsdvr_separable_sdf_grad(float *table_grad, uint32_t reso, float *x_grad, float *y_grad, float *z_grad,
+                             float *offset_grad, cudaStream_t stream);
 
 /* Workspace bytes for qsdvr_render_* with these args on the current device (mode, storage
  * and transmittance select the kernel; independent of ray_count).  One workspace must not

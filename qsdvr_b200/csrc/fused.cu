@@ -94,7 +94,9 @@ struct Params {
     uint32_t n;
     uint32_t R;
     float interval, k, volume_offset;
-    const void *sdf;   // [R^3][8]
+    const void *sdf;   // [R^3][8], or null with sep
+    const float4 *sep; // separable SDF: [3][R] (a0, a3, a6, 0) per axis index, then (off3, 0, 0, 0)
+    float4 *sep_grad;  // its gradient, same layout (the last entry unused)
     const void *data;  // [(R+1)^3][32]
     float *color;
     const float *target;
@@ -152,6 +154,43 @@ struct Store<__nv_bfloat16> {
         return make_float4(bf_lo(r.x), bf_hi(r.x), bf_lo(r.y), bf_hi(r.y));
     }
 };
+
+__device__ __forceinline__ void red_cell(float *g8, uint32_t cell, const float *g) {
+    float *b = g8 + 8ull * cell;
+    red4(b, make_float4(g[0], g[1], g[2], g[3]));
+    red4(b + 4, make_float4(g[4], g[5], g[6], 0.0f));
+}
+
+// Separable SDF (models/render.py:172-207): cell (x, y, z) has coefficients
+// (x0[x], y1[y], z2[z], x3[x], y4[y], z5[z], ((x6[x] + y6[y]) + z6[z]) + off3), the sum in the
+// order kernel/surface.cu:3-24 materialises it, so a cell is bit-identical to the dense grid
+// LayerToGrid would write.  The per-axis rows are O(R) and stay in L1/L2.
+__device__ __forceinline__ void sep_cell(const float4 *sep, uint32_t R, const CellPoint &c, float *a) {
+    const float4 x = sep[c.cx], y = sep[R + c.cy], z = sep[2 * R + c.cz];
+    const float off3 = sep[3 * R].x;
+    a[0] = x.x; a[1] = y.x; a[2] = z.x;
+    a[3] = x.y; a[4] = y.y; a[5] = z.y;
+    a[6] = __fadd_rn(__fadd_rn(__fadd_rn(x.z, y.z), z.z), off3);
+}
+
+// Its adjoint: one 16-byte RED per axis row.  The off3 gradient (the sum of every cell's g6)
+// is recovered from the x rows' g6 sums by the reverse recurrence, so it needs no atomics.
+__device__ __forceinline__ void sep_red(float4 *sg, uint32_t R, const CellPoint &c, const float *g) {
+    red4(reinterpret_cast<float *>(sg + c.cx), make_float4(g[0], g[3], g[6], 0.0f));
+    red4(reinterpret_cast<float *>(sg + R + c.cy), make_float4(g[1], g[4], g[6], 0.0f));
+    red4(reinterpret_cast<float *>(sg + 2 * R + c.cz), make_float4(g[2], g[5], g[6], 0.0f));
+}
+
+template <typename S>
+__device__ __forceinline__ void load_cell(const Params &p, const CellPoint &c, float *a) {
+    if (p.sep) sep_cell(p.sep, p.R, c, a);
+    else Store<S>::cell(p.sdf, (uint32_t)c.index, a);
+}
+
+__device__ __forceinline__ void scatter_cell(const Params &p, const CellPoint &c, const float *g) {
+    if (p.sep_grad) sep_red(p.sep_grad, p.R, c, g);
+    else red_cell(p.sdf_grad, (uint32_t)c.index, g);
+}
 
 __device__ __forceinline__ float lerp_ref(float a, float b, float x) { return a * (1 - x) + b * x; }
 __device__ __forceinline__ float4 lerp4(float4 a, float4 b, float x) {
@@ -275,7 +314,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     float s1 = 0.0f;
     if (live) {
         if (cell_in_grid(s.c1, R)) {
-            Store<S>::cell(p.sdf, (uint32_t)s.c1.index, a1);
+            load_cell<S>(p, s.c1, a1);
             s1 = checked_sdf<kCompat>(a1, s.c1.u, (float)R);
         } else {
             ok = false;
@@ -287,7 +326,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
             to_cell(tl ? at_t(o, d, tl[i]) : march(o, d, (float)i, p.interval), p.volume_offset, R);
         if (cell_in_grid(c0, R)) {
             float a0[7];
-            Store<S>::cell(p.sdf, (uint32_t)c0.index, a0);
+            load_cell<S>(p, c0, a0);
             s0 = checked_sdf<kCompat>(a0, c0.u, (float)R);
         } else {
             ok = false;
@@ -300,7 +339,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
                    p.volume_offset, R);
     float ar[7];
     if (live && cell_in_grid(s.cr, R)) {
-        Store<S>::cell(p.sdf, (uint32_t)s.cr.index, ar);
+        load_cell<S>(p, s.cr, ar);
         s.nrm = sample_normal<kCompat>(ar, s.cr.u);
     } else {
         ok = false;
@@ -390,7 +429,7 @@ __device__ __forceinline__ void eval_alpha(const Params &p, uint32_t r, f3 o, f3
     if (live) {
         if (cell_in_grid(c1, R)) {
             float a1[7];
-            Store<S>::cell(p.sdf, (uint32_t)c1.index, a1);
+            load_cell<S>(p, c1, a1);
             s1 = checked_sdf<kCompat>(a1, c1.u, (float)R);
         } else {
             ok = false;
@@ -402,7 +441,7 @@ __device__ __forceinline__ void eval_alpha(const Params &p, uint32_t r, f3 o, f3
             to_cell(tl ? at_t(o, d, tl[i]) : march(o, d, (float)i, p.interval), p.volume_offset, R);
         if (cell_in_grid(c0, R)) {
             float a0[7];
-            Store<S>::cell(p.sdf, (uint32_t)c0.index, a0);
+            load_cell<S>(p, c0, a0);
             s0 = checked_sdf<kCompat>(a0, c0.u, (float)R);
         } else {
             ok = false;
@@ -496,11 +535,6 @@ __device__ __forceinline__ void scatter_tile(const Params &p, const float *tile,
     }
 }
 
-__device__ __forceinline__ void red_cell(float *g8, uint32_t cell, const float *g) {
-    float *b = g8 + 8ull * cell;
-    red4(b, make_float4(g[0], g[1], g[2], g[3]));
-    red4(b + 4, make_float4(g[4], g[5], g[6], 0.0f));
-}
 
 template <bool kCompat, typename S, int kPass, bool kLogT, int kDeg>
 __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kernel(const Params p) {
@@ -665,30 +699,30 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                     // SDF sample i+1 and, for the ray's first lane, SDF sample 0
                     const float gs1 = dl * d_next + (i + 1 < nr ? from_next : 0.0f);
                     float a1[7], gq[7];
-                    Store<S>::cell(p.sdf, (uint32_t)s.c1.index, a1);
+                    load_cell<S>(p, s.c1, a1);
                     quad_sdf_grad(a1, s.c1.u, (float)p.R, gs1, gq);
                     // rgb gradient -> shader backward (data gradient into the tile, normal gradient)
                     const f3 grgb{g.x * T * a, g.y * T * a, g.z * T * a};
                     // data gradient written over the data row (every read precedes its write)
                     const f3 gn = shade_any_backward_inplace<kCompat, kDeg>(grgb, s.nrm, d, tile + lane * kRow, s.spec);
                     float ar[7], gr[6];
-                    Store<S>::cell(p.sdf, (uint32_t)s.cr.index, ar);
+                    load_cell<S>(p, s.cr, ar);
                     sample_normal_grad<kCompat>(ar, s.cr.u, gn, gr);
                     if (s.cr.index == s.c1.index) {
 #pragma unroll
                         for (int t = 0; t < 6; ++t) gq[t] += gr[t];
-                        red_cell(p.sdf_grad, (uint32_t)s.c1.index, gq);
+                        scatter_cell(p, s.c1, gq);
                     } else {
-                        red_cell(p.sdf_grad, (uint32_t)s.c1.index, gq);
+                        scatter_cell(p, s.c1, gq);
                         const float g7[7] = {gr[0], gr[1], gr[2], gr[3], gr[4], gr[5], 0.0f};
-                        red_cell(p.sdf_grad, (uint32_t)s.cr.index, g7);
+                        scatter_cell(p, s.cr, g7);
                     }
                     if (i == 0) {
                         const CellPoint c0 = to_cell(march(o, d, 0.0f, p.interval), p.volume_offset, p.R);
                         float a0[7], g0[7];
-                        Store<S>::cell(p.sdf, (uint32_t)c0.index, a0);
+                        load_cell<S>(p, c0, a0);
                         quad_sdf_grad(a0, c0.u, (float)p.R, mine_this, g0);
-                        red_cell(p.sdf_grad, (uint32_t)c0.index, g0);
+                        scatter_cell(p, c0, g0);
                     }
                 }
                 __syncwarp();
@@ -798,6 +832,8 @@ int launch(const qsdvr_render_args *a, cudaStream_t stream) {
     p.k = a->logistic_coef;
     p.volume_offset = (float)a->reso / 2.0f;
     p.sdf = a->sdf_grid;
+    p.sep = reinterpret_cast<const float4 *>(a->sdf_layers);
+    p.sep_grad = a->sdf_layers ? reinterpret_cast<float4 *>(a->sdf_layers_grad) : nullptr;
     p.data = a->data;
     p.color = a->color;
     p.target = a->target;
@@ -832,7 +868,8 @@ int launch(const qsdvr_render_args *a, cudaStream_t stream) {
 
 int validate(const qsdvr_render_args *a, int pass) {
     if (!a) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null args");
-    if (a->ray_count && (!a->rays || !a->origin || !a->dir || !a->sdf_grid || !a->data))
+    const bool sep = a->sdf_layers != nullptr;
+    if (a->ray_count && (!a->rays || !a->origin || !a->dir || !(a->sdf_grid || sep) || !a->data))
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null ray or grid pointer");
     if (a->reso == 0 || a->reso > 1290)
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: reso %u out of range", a->reso);
@@ -847,10 +884,11 @@ int validate(const qsdvr_render_args *a, int pass) {
     if (a->transmittance != QSDVR_TRANSMITTANCE_PRODUCT && a->transmittance != QSDVR_TRANSMITTANCE_LOG)
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: bad transmittance form %d", a->transmittance);
     if (!(a->interval > 0.0f)) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: interval must be > 0");
-    if (!aligned(a->sdf_grid, 16) || !aligned(a->data, 16) || !aligned(a->rays, 16))
-        return set_error(QSDVR_ERR_ALIGNMENT, "render: rays, sdf_grid and data need 16-byte alignment");
+    if (!aligned(a->sdf_grid, 16) || !aligned(a->sdf_layers, 16) || !aligned(a->data, 16) || !aligned(a->rays, 16))
+        return set_error(QSDVR_ERR_ALIGNMENT, "render: rays, SDF and data need 16-byte alignment");
+    float *const sdf_g = sep ? a->sdf_layers_grad : a->sdf_grad;
     if (pass != kForward && a->ray_count &&
-        (!a->sdf_grad || !a->data_grad || !aligned(a->sdf_grad, 16) || !aligned(a->data_grad, 16)))
+        (!sdf_g || !a->data_grad || !aligned(sdf_g, 16) || !aligned(a->data_grad, 16)))
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: gradient buffers missing or not 16-byte aligned");
     if (pass != kBackward && a->ray_count && !a->color)
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null color output");

@@ -164,6 +164,57 @@ __global__ void layer_grad_reverse_kernel(float *__restrict__ xg, float *__restr
     offset_grad[axis] = a3[0];
 }
 
+// ---- separable SDF tables for the fused renderer ---------------------------------------------
+// tables [3R+1] float4: axis a, index i -> (a0, a3, a6, 0) of the per-axis recurrences (the
+// same arithmetic as layer_tables_kernel), then (off3, 0, 0, 0).
+__global__ void separable_tables_kernel(const float *__restrict__ x0, const float *__restrict__ y1,
+                                        const float *__restrict__ z2, const float *__restrict__ offset, uint32_t R,
+                                        float4 *__restrict__ tables) {
+    const int axis = threadIdx.x;
+    if (axis == 3) tables[3 * R] = make_float4(offset[3], 0.0f, 0.0f, 0.0f);
+    if (axis >= 3) return;
+    const float *a0 = axis == 0 ? x0 : (axis == 1 ? y1 : z2);
+    float4 *t = tables + axis * R;
+    float p3 = offset[axis], p6 = 0.0f;
+    t[0] = make_float4(a0[0], p3, p6, 0.0f);
+    for (uint32_t i = 1; i < R; ++i) {
+        const float c3 = __fadd_rn(__fadd_rn(__fmul_rn(2.0f, a0[i - 1]), __fmul_rn(2.0f, a0[i])), p3);
+        const float c6 =
+            __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(3.0f, a0[i - 1]), a0[i]), __fmul_rn(2.0f, p3)), p6);
+        t[i] = make_float4(a0[i], c3, c6, 0.0f);
+        p3 = c3;
+        p6 = c6;
+    }
+}
+
+// Adjoint (kernel/surface.cu:301-334 on the per-axis sums the fused renderer accumulated):
+// reverse recurrences in place over the table gradient, then the layer and offset gradients.
+// offset[3]'s gradient is the sum of every cell's g6 = the x axis' a6 chain summed to index 0.
+__global__ void separable_grad_kernel(float4 *__restrict__ tg, uint32_t R, float *__restrict__ x_grad,
+                                      float *__restrict__ y_grad, float *__restrict__ z_grad,
+                                      float *__restrict__ offset_grad) {
+    const int axis = threadIdx.x;
+    if (axis >= 3) return;
+    float4 *t = tg + axis * R;  // (.x a0, .y a3, .z a6)
+    for (uint32_t i = R - 1; i > 0; --i) {
+        const float a6 = t[i].z;
+        t[i].x = __fadd_rn(t[i].x, a6);
+        t[i - 1].x = __fadd_rn(t[i - 1].x, __fmul_rn(3.0f, a6));
+        t[i - 1].y = __fadd_rn(t[i - 1].y, __fmul_rn(2.0f, a6));
+        t[i - 1].z = __fadd_rn(t[i - 1].z, a6);
+    }
+    for (uint32_t i = R - 1; i > 0; --i) {
+        const float a3 = t[i].y;
+        t[i].x = __fadd_rn(t[i].x, __fmul_rn(2.0f, a3));
+        t[i - 1].x = __fadd_rn(t[i - 1].x, __fmul_rn(2.0f, a3));
+        t[i - 1].y = __fadd_rn(t[i - 1].y, a3);
+    }
+    float *out = axis == 0 ? x_grad : (axis == 1 ? y_grad : z_grad);
+    for (uint32_t i = 0; i < R; ++i) out[i] = t[i].x;
+    offset_grad[axis] = t[0].y;
+    if (axis == 0) offset_grad[3] = t[0].z;
+}
+
 // ---- SDF / normal samples ------------------------------------------------------------------
 
 __device__ __forceinline__ bool cell_ok(int32_t idx, uint64_t cells) {
@@ -319,6 +370,30 @@ extern "C" int qsdvr_layer_to_grid_backward(const float *grad7, uint32_t reso, f
                                                                              acc, offset_grad + 3);
     layer_grad_reverse_kernel<<<1, 32, 0, stream>>>(x_grad, y_grad, z_grad, acc, offset_grad, reso);
     return check_launch("qsdvr_layer_to_grid_backward");
+}
+
+extern "C" int qsdvr_separable_sdf_tables(const float *x_layer, const float *y_layer, const float *z_layer,
+                                          const float *offset, uint32_t reso, float *tables, cudaStream_t stream) {
+    if (!x_layer || !y_layer || !z_layer || !offset || !tables)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_separable_sdf_tables: null pointer");
+    if (reso == 0 || reso > kMaxReso)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_separable_sdf_tables: reso %u out of range", reso);
+    if (!aligned(tables, 16)) return set_error(QSDVR_ERR_ALIGNMENT, "qsdvr_separable_sdf_tables: tables alignment");
+    separable_tables_kernel<<<1, 32, 0, stream>>>(x_layer, y_layer, z_layer, offset, reso,
+                                                  reinterpret_cast<float4 *>(tables));
+    return check_launch("qsdvr_separable_sdf_tables");
+}
+
+extern "C" int qsdvr_separable_sdf_grad(float *table_grad, uint32_t reso, float *x_grad, float *y_grad,
+                                        float *z_grad, float *offset_grad, cudaStream_t stream) {
+    if (!table_grad || !x_grad || !y_grad || !z_grad || !offset_grad)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_separable_sdf_grad: null pointer");
+    if (reso == 0 || reso > kMaxReso)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_separable_sdf_grad: reso %u out of range", reso);
+    if (!aligned(table_grad, 16)) return set_error(QSDVR_ERR_ALIGNMENT, "qsdvr_separable_sdf_grad: alignment");
+    separable_grad_kernel<<<1, 32, 0, stream>>>(reinterpret_cast<float4 *>(table_grad), reso, x_grad, y_grad, z_grad,
+                                                offset_grad);
+    return check_launch("qsdvr_separable_sdf_grad");
 }
 
 extern "C" int qsdvr_sample_sdf_forward(float *out, const float *grid7, const float *points, const int32_t *index,

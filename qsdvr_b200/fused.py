@@ -13,6 +13,7 @@ Ray batches are the reference's per-ray tables: ``rays`` int32 [N,4] (RayInfo),
 from __future__ import annotations
 
 import ctypes
+import math
 
 import torch
 from torch import autograd, nn
@@ -31,13 +32,16 @@ class RenderArgs(ctypes.Structure):
                 ("logistic_coef", F32), ("mode", I32), ("storage", I32), ("transmittance", I32), ("sh_degree", I32),
                 ("sdf_grid", P), ("data", P), ("color", P), ("target", P), ("grad_color", P), ("sdf_grad", P),
                 ("data_grad", P), ("loss", P), ("grad_scale", F32), ("workspace", P), ("workspace_bytes", ctypes.c_uint64),
-                ("tlist", P), ("sample_alpha", P), ("sample_capacity", ctypes.c_uint64)]
+                ("sdf_layers", P), ("sdf_layers_grad", P), ("tlist", P), ("sample_alpha", P),
+                ("sample_capacity", ctypes.c_uint64)]
 
 
 _lib.extra_signatures({
     "qsdvr_render_forward": [ctypes.POINTER(RenderArgs), P],
     "qsdvr_render_backward": [ctypes.POINTER(RenderArgs), P],
     "qsdvr_render_train": [ctypes.POINTER(RenderArgs), P],
+    "qsdvr_separable_sdf_tables": [P, P, P, P, U32, P, P],
+    "qsdvr_separable_sdf_grad": [P, U32, P, P, P, P, P],
 }, {"qsdvr_render_workspace_size": [ctypes.POINTER(RenderArgs)]})
 
 _workspaces: dict = {}
@@ -94,14 +98,27 @@ def _grid_storage(sdf_grid, data, R):
 
 def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat", transmittance="product",
               color=None, target=None, grad_color=None, sdf_grad=None, data_grad=None, loss=None,
-              grad_scale=0.0, persistent=True, tlist=None, sample_alpha=None) -> RenderArgs:
+              grad_scale=0.0, persistent=True, tlist=None, sample_alpha=None, sdf_layers=None,
+              sdf_layers_grad=None) -> RenderArgs:
     dev, n = _check_batch(rays, origin, direction)
     a = RenderArgs()
     a.rays, a.origin, a.dir = _ptr(rays), _ptr(origin), _ptr(direction)
     a.ray_count, a.reso = n, int(reso)
     a.interval, a.logistic_coef = float(interval), float(k)
     a.mode = MODES[mode]
-    a.storage = _grid_storage(sdf_grid, data, int(reso))
+    if sdf_layers is not None:
+        rows = 3 * int(reso) + 1
+        for t, nm in ((sdf_layers, "sdf_layers"), (sdf_layers_grad, "sdf_layers_grad")):
+            if t is not None and (t.device != dev or t.dtype != torch.float32 or t.shape != (rows, 4)
+                                  or not t.is_contiguous()):
+                raise ValueError(f"{nm} must be a contiguous float32 [{rows},4] tensor on {dev}")
+        if data.dtype not in (torch.float32, torch.bfloat16) or not data.is_contiguous():
+            raise TypeError("data must be a contiguous float32 or bfloat16 tensor")
+        sh_degree_of(data, int(reso))
+        a.storage = STORAGE["bf16" if data.dtype == torch.bfloat16 else "f32"]
+        a.sdf_layers, a.sdf_layers_grad = _ptr(sdf_layers), _ptr(sdf_layers_grad)
+    else:
+        a.storage = _grid_storage(sdf_grid, data, int(reso))
     a.transmittance = TRANSMITTANCE[transmittance]
     a.sh_degree = sh_degree_of(data, int(reso))
     a.sdf_grid, a.data = _ptr(sdf_grid), _ptr(data)
@@ -129,48 +146,56 @@ def _stream(dev):
 
 
 def render_forward(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat",
-                   transmittance="product", color=None, persistent=True, tlist=None, sample_alpha=None):
+                   transmittance="product", color=None, persistent=True, tlist=None, sample_alpha=None,
+                   sdf_layers=None):
     """Colour of every ray [N,3].  ``tlist`` [N,33]: render at those SDF positions (32 render
     samples per ray at their midpoints) instead of the uniform march; ``sample_alpha``: also
-    write every render sample's alpha at the ray's render offset."""
+    write every render sample's alpha at the ray's render offset; ``sdf_layers`` (with
+    ``sdf_grid`` None): the separable SDF tables of ``separable_tables``."""
     dev, n = _check_batch(rays, origin, direction)
     if color is None:
         color = torch.empty((n, 3), dtype=torch.float32, device=dev)
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color,
-                  persistent=persistent, tlist=tlist, sample_alpha=sample_alpha)
+                  persistent=persistent, tlist=tlist, sample_alpha=sample_alpha, sdf_layers=sdf_layers)
     with torch.cuda.device(dev):
         call("qsdvr_render_forward", ctypes.byref(a), _stream(dev))
     return color
 
 
 def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
-                    mode="compat", transmittance="product", persistent=True, tlist=None):
-    """Accumulate dL/d(sdf_grid) and dL/d(data) (fp32) for a given dL/dcolor."""
+                    mode="compat", transmittance="product", persistent=True, tlist=None, sdf_layers=None):
+    """Accumulate dL/d(sdf_grid) and dL/d(data) (fp32) for a given dL/dcolor.  With
+    ``sdf_layers``, ``sdf_grad`` is the tables' gradient ([3R+1,4], see ``separable_grad``)."""
     dev, n = _check_batch(rays, origin, direction)
-    for t, nm, shape in ((sdf_grad, "sdf_grad", sdf_grid.numel()), (data_grad, "data_grad", data.numel())):
+    sdf_src = sdf_layers if sdf_layers is not None else sdf_grid
+    for t, nm, shape in ((sdf_grad, "sdf_grad", sdf_src.numel()), (data_grad, "data_grad", data.numel())):
         if t.dtype != torch.float32 or t.numel() != shape or t.device != dev or not t.is_contiguous():
             raise ValueError(f"{nm} must be a contiguous float32 tensor shaped like its grid")
     g = grad_color.contiguous().float()
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, grad_color=g,
-                  sdf_grad=sdf_grad, data_grad=data_grad, persistent=persistent, tlist=tlist)
+                  sdf_grad=None if sdf_layers is not None else sdf_grad, data_grad=data_grad,
+                  persistent=persistent, tlist=tlist, sdf_layers=sdf_layers,
+                  sdf_layers_grad=sdf_grad if sdf_layers is not None else None)
     with torch.cuda.device(dev):
         call("qsdvr_render_backward", ctypes.byref(a), _stream(dev))
 
 
 def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
                  mode="compat", transmittance="product", loss=None, color=None, persistent=True, tlist=None,
-                 sample_alpha=None):
+                 sample_alpha=None, sdf_layers=None):
     """Forward + MSE (mean over N x 3) + backward in one launch.  Returns (color, loss_sum)
-    where loss_sum accumulates sum |color - target|^2 (divide by 3N for the mean)."""
+    where loss_sum accumulates sum |color - target|^2 (divide by 3N for the mean).  With
+    ``sdf_layers``, ``sdf_grad`` is the tables' gradient ([3R+1,4])."""
     dev, n = _check_batch(rays, origin, direction)
     if color is None:
         color = torch.empty((n, 3), dtype=torch.float32, device=dev)
     if loss is None:
         loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    sep = sdf_layers is not None
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color,
-                  target=target.contiguous(), sdf_grad=sdf_grad, data_grad=data_grad, loss=loss,
+                  target=target.contiguous(), sdf_grad=None if sep else sdf_grad, data_grad=data_grad, loss=loss,
                   grad_scale=2.0 / (3.0 * max(n, 1)), persistent=persistent, tlist=tlist,
-                  sample_alpha=sample_alpha)
+                  sample_alpha=sample_alpha, sdf_layers=sdf_layers, sdf_layers_grad=sdf_grad if sep else None)
     with torch.cuda.device(dev):
         call("qsdvr_render_train", ctypes.byref(a), _stream(dev))
     return color, loss
@@ -278,3 +303,108 @@ class _Bf16Render(autograd.Function):
         render_backward(grad_color, rays, origin, direction, sdf_bf16, data_bf16, m.reso, m.interval, m.logisticCoef,
                         sg, dg, m.mode, m.transmittance)
         return sg, dg, None, None, None, None, None, None
+
+
+# ----------------------------------------------------------------------------- separable SDF
+
+def separable_tables(x_layer, y_layer, z_layer, offset) -> torch.Tensor:
+    """[3R+1, 4] tables of the separable quadric grid (models/render.py:172-207 layers +
+    offset; the per-axis recurrences of LayerToGridForward, kernel/surface.cu:161-178)."""
+    R = x_layer.numel()
+    dev = x_layer.device
+    for t, nm, nn_ in ((x_layer, "x_layer", R), (y_layer, "y_layer", R), (z_layer, "z_layer", R), (offset, "offset", 4)):
+        if not t.is_cuda or t.device != dev or t.dtype != torch.float32 or t.numel() != nn_ or not t.is_contiguous():
+            raise ValueError(f"{nm} must be a contiguous float32 CUDA tensor of {nn_} values on {dev}")
+    out = torch.empty((3 * R + 1, 4), dtype=torch.float32, device=dev)
+    with torch.cuda.device(dev):
+        call("qsdvr_separable_sdf_tables", _ptr(x_layer), _ptr(y_layer), _ptr(z_layer), _ptr(offset), R, _ptr(out),
+             _stream(dev))
+    return out
+
+
+def separable_grad(table_grad: torch.Tensor):
+    """(x, y, z layer gradients [R], offset gradient [4]) from the tables' gradient, which
+    the call consumes (the reverse recurrences run in place)."""
+    R = (table_grad.shape[0] - 1) // 3
+    dev = table_grad.device
+    if table_grad.dtype != torch.float32 or table_grad.shape != (3 * R + 1, 4) or not table_grad.is_contiguous():
+        raise ValueError("table_grad must be a contiguous float32 [3R+1,4] tensor")
+    xg, yg, zg = (torch.empty(R, dtype=torch.float32, device=dev) for _ in range(3))
+    og = torch.empty(4, dtype=torch.float32, device=dev)
+    with torch.cuda.device(dev):
+        call("qsdvr_separable_sdf_grad", _ptr(table_grad), R, _ptr(xg), _ptr(yg), _ptr(zg), _ptr(og), _stream(dev))
+    return xg, yg, zg, og
+
+
+class _SeparableRender(autograd.Function):
+    @staticmethod
+    def forward(ctx, x_layer, y_layer, z_layer, offset, data, rays, origin, direction, cfg):
+        reso, interval, k, mode, transmittance = cfg
+        tables = separable_tables(x_layer.detach(), y_layer.detach(), z_layer.detach(), offset.detach())
+        color = render_forward(rays, origin, direction, None, data.detach(), reso, interval, k, mode, transmittance,
+                               sdf_layers=tables)
+        ctx.save_for_backward(tables, data, rays, origin, direction)
+        ctx.cfg = cfg
+        return color
+
+    @staticmethod
+    def backward(ctx, grad_color):
+        tables, data, rays, origin, direction = ctx.saved_tensors
+        reso, interval, k, mode, transmittance = ctx.cfg
+        tg = torch.zeros_like(tables)
+        dg = torch.zeros(data.shape, dtype=torch.float32, device=data.device)
+        render_backward(grad_color, rays, origin, direction, None, data.detach(), reso, interval, k, tg, dg, mode,
+                        transmittance, sdf_layers=tables)
+        xg, yg, zg, og = separable_grad(tg)
+        return xg, yg, zg, og, dg.to(data.dtype), None, None, None, None
+
+
+class SeparableRenderGrid(nn.Module):
+    """The reference RenderGrid (models/render.py:172-237: QuadricGrid layers + offset and the
+    [(R+1)^3,32] appearance grid, same initial values) rendered and differentiated by the fused
+    kernels.  The [R^3,7] cell grid is never materialised: the kernels assemble each cell from
+    O(R) per-axis tables and reduce its gradient back into them."""
+
+    def __init__(self, reso: int = 128, logisticCoef: float = 5.0, interval: float = 4.0 / 256, mode: str = "compat",
+                 transmittance: str = "product", device="cuda"):
+        super().__init__()
+        self.reso, self.interval, self.mode, self.transmittance = reso, interval, mode, transmittance
+        self.logisticCoef = logisticCoef
+        dev = torch.device(device)
+        self.xLayer = nn.Parameter(torch.ones(reso, dtype=torch.float32, device=dev))
+        self.yLayer = nn.Parameter(torch.ones(reso, dtype=torch.float32, device=dev))
+        self.zLayer = nn.Parameter(torch.ones(reso, dtype=torch.float32, device=dev))
+        c = -reso  # models/render.py:187-192
+        self.offset = nn.Parameter(torch.tensor([-2.0 * c, -2.0 * c, -2.0 * c, math.sqrt(3 * c * c)],
+                                                dtype=torch.float32, device=dev))
+        data = torch.zeros(((reso + 1) ** 3, 32), dtype=torch.float32, device=dev)
+        data[:, 31] = 1  # models/render.py:215-223
+        data[:, 30] = 0.1
+        data[:, 27:30] = 1
+        data[:, 0:3] = 0.5
+        self.renderData = nn.Parameter(data)
+
+    def cfg(self):
+        return (self.reso, self.interval, self.logisticCoef, self.mode, self.transmittance)
+
+    def forward(self, rays, origin, direction):
+        return _SeparableRender.apply(self.xLayer, self.yLayer, self.zLayer, self.offset, self.renderData, rays, origin,
+                                      direction, self.cfg())
+
+    def train_step(self, target, rays, origin, direction, loss=None):
+        """Forward + MSE + backward in one fused launch; accumulates into the parameters' .grad.
+        Returns (colour, loss_sum)."""
+        tables = separable_tables(self.xLayer.detach(), self.yLayer.detach(), self.zLayer.detach(),
+                                  self.offset.detach())
+        tg = torch.zeros_like(tables)
+        if self.renderData.grad is None:
+            self.renderData.grad = torch.zeros_like(self.renderData)
+        color, loss = render_train(target, rays, origin, direction, None, self.renderData.detach(), self.reso,
+                                   self.interval, self.logisticCoef, tg, self.renderData.grad, self.mode,
+                                   self.transmittance, loss=loss, sdf_layers=tables)
+        for p, g in zip((self.xLayer, self.yLayer, self.zLayer, self.offset), separable_grad(tg)):
+            p.grad = g if p.grad is None else p.grad.add_(g)
+        return color, loss
+
+    def set_logisticCoef(self, logisticCoef):
+        self.logisticCoef = logisticCoef
