@@ -382,7 +382,7 @@ def proposal_comparison(steps: int):
     about the render time of one plain step; the first 20% of its steps use the uniform march
     while the network learns).  rays/s is device time of the forward + backward part of the
     steps (for the proposal: coarse MLP, sampler, online network update and the fused train
-    launch); PSNR is on 65536 held-out rays, judged by the uniform march."""
+    launch); PSNR is on 65536 held-out rays rendered by the uniform march."""
     from qsdvr_b200 import train
 
     a = train.parser().parse_args([])
@@ -409,7 +409,7 @@ def proposal_comparison(steps: int):
             "delta_psnr": round(plain["heldout_psnr_end"] - prop["heldout_psnr_end"], 3),
             "psnr_proposal_render": prop["heldout_psnr_end_proposal_render"],
             "delta_psnr_method": round(plain["heldout_psnr_end"] - prop["heldout_psnr_end_proposal_render"], 3),
-            "judge": "held-out rays vs ground truth: delta_psnr with both models rendered by the 256-sample "
+            "psnr_reference": "held-out rays vs ground truth: delta_psnr with both models rendered by the 256-sample "
                      "uniform march, delta_psnr_method with each model rendered by its own method"}
 
 

@@ -6,7 +6,8 @@ read, Adam state).  It is trained online on the renderer's own per-sample opacit
 uniform-march forward writes the alpha of every render sample, ``targets`` turns them into
 (position, density) pairs and ``train_step`` fits the density bound.  ``sample`` gives each
 ray its 33 fine SDF positions; ``render`` renders with them (32 render samples per ray).
-The uniform march stays the fallback (an untrained network) and the judge of the result.
+The uniform march stays the fallback (an untrained network) and the reference its PSNR is
+measured against.
 """
 from __future__ import annotations
 

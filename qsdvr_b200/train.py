@@ -13,7 +13,7 @@ their gradients and Adam state is O(rays).
 MLP evaluations place them) instead of the uniform march (after ``--proposal-warmup`` steps
 with it).  The network is trained online every step on the per-sample alphas of a
 uniform-march forward over part of the batch.
-Held-out PSNR is always measured with the uniform march (the judge).
+Held-out PSNR is always measured with the uniform march.
 """
 from __future__ import annotations
 

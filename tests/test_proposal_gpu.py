@@ -296,8 +296,8 @@ def _psnr(a, b):
 def test_trained_proposal_beats_same_budget_without_it(prop):
     """Train the proposal MLP on the renderer's own per-sample alphas, then render a held-out
     view with 64 coarse MLP points + 32 fine samples and with 32 evenly spaced samples (the
-    method without the network, same render budget).  The 512-sample uniform march is the
-    judge: the trained network must be closer to it by a wide margin."""
+    method without the network, same render budget).  Both are measured against the
+    512-sample uniform march: the trained network must be closer to it by a wide margin."""
     from qsdvr_b200 import fused, scenes
 
     R, k = 64, 50.0
@@ -321,11 +321,11 @@ def test_trained_proposal_beats_same_budget_without_it(prop):
     assert loss < 0.25 * first
     held = _camera((2.3, 2.9, 1.9), 100, 138.9, interval, R)
     args = (held.rayList, held.originList, held.dirList)
-    judge = fused.render_forward(*args, grid8, data, R, interval, k, "fixed")
+    full = fused.render_forward(*args, grid8, data, R, interval, k, "fixed")
     t_prop = net.sample(*args, interval)
     img_prop = fused.render_forward(*args, grid8, data, R, interval, k, "fixed", tlist=t_prop)
     img_flat = fused.render_forward(*args, grid8, data, R, interval, k, "fixed",
                                     tlist=prop.uniform_tlist(held.rayList, interval))
-    p_prop, p_flat = _psnr(img_prop, judge), _psnr(img_flat, judge)
+    p_prop, p_flat = _psnr(img_prop, full), _psnr(img_flat, full)
     print(f"PSNR vs 512-sample march: proposal {p_prop:.2f} dB, uniform-32 {p_flat:.2f} dB")
     assert p_prop > p_flat + 3.0
