@@ -6,9 +6,10 @@
 // Work mapping (one warp per ray, 32 render samples per "chunk"):
 //   * lane i owns render sample i of the chunk: its positions (bit-exact with
 //     GenerateRayPoints), quadric cells, SDF values, normal, alpha and shading;
-//   * the 32-channel appearance rows are gathered by groups of 8 lanes (one float4 or
-//     4 x bf16 each), so every load covers whole 128-byte (64-byte bf16) vertex rows,
-//     interpolated and staged in a per-warp shared-memory tile [32][36] floats
+//   * the 32-channel appearance rows are gathered with 16-byte loads by groups of 8 lanes
+//     (one float4 each) or 4 lanes (bf16 x 8 each), so every load covers whole 128-byte
+//     (64-byte bf16) vertex rows, interpolated and staged in a per-warp shared-memory
+//     tile [32][36] floats
 //     (row stride 36 keeps both the row-wise and the lane-wise float4 accesses
 //     conflict-free);
 //   * transmittance is an exclusive prefix product (or a compensated prefix sum of
@@ -148,12 +149,23 @@ struct Store<__nv_bfloat16> {
         a[0] = bf_lo(r.x); a[1] = bf_hi(r.x); a[2] = bf_lo(r.y); a[3] = bf_hi(r.y);
         a[4] = bf_lo(r.z); a[5] = bf_hi(r.z); a[6] = bf_lo(r.w);
     }
-    __device__ static float4 quad(const void *d, uint32_t v, int q, int C) {
-        const uint2 r =
-            *reinterpret_cast<const uint2 *>(static_cast<const __nv_bfloat16 *>(d) + (uint64_t)C * v + 4 * q);
-        return make_float4(bf_lo(r.x), bf_hi(r.x), bf_lo(r.y), bf_hi(r.y));
+    // channels [8q, 8q + 8) of vertex v: one 16-byte load (bf16 x 8)
+    __device__ static uint4 oct(const void *d, uint32_t v, int q, int C) {
+        return *reinterpret_cast<const uint4 *>(static_cast<const __nv_bfloat16 *>(d) + (uint64_t)C * v + 8 * q);
     }
 };
+
+// Lanes of the appearance gather: each lane loads 16 bytes of a vertex row per corner (a
+// float4 of fp32 storage, 8 x bf16 of bf16 storage), so kLanes lanes cover one row and a warp
+// instruction fetches kPerStep samples' rows.
+template <typename S, int kDeg>
+struct GatherLanes {
+    static constexpr int kC = ShLayout<kDeg>::kChannels;
+    static constexpr int kCh = 16 / (int)sizeof(S);  // channels per lane
+    static constexpr int kLanes = kC / kCh;
+    static constexpr int kPerStep = kWarp / kLanes;
+};
+
 
 __device__ __forceinline__ void red_cell(float *g8, uint32_t cell, const float *g) {
     float *b = g8 + 8ull * cell;
@@ -197,6 +209,15 @@ __device__ __forceinline__ float4 lerp4(float4 a, float4 b, float x) {
     return make_float4(lerp_ref(a.x, b.x, x), lerp_ref(a.y, b.y, x), lerp_ref(a.z, b.z, x), lerp_ref(a.w, b.w, x));
 }
 __device__ __forceinline__ float4 scale4(float4 v, float w) { return make_float4(v.x * w, v.y * w, v.z * w, v.w * w); }
+// Per-channel lerp_ref of two bf16 x 8 vectors.
+__device__ __forceinline__ void lerp_bf8(uint4 a, uint4 b, float x, float *o) {
+    const uint32_t av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        o[2 * t] = lerp_ref(bf_lo(av[t]), bf_lo(bv[t]), x);
+        o[2 * t + 1] = lerp_ref(bf_hi(av[t]), bf_hi(bv[t]), x);
+    }
+}
 
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
@@ -378,8 +399,55 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
         }
         return;
     }
-    // gather: groups of kL lanes fetch one sample's 8 corner rows, kPS samples per step
     const uint32_t sy = R1, sz = R1 * R1;
+    if constexpr (sizeof(S) == 2) {
+        // bf16 storage: groups of kGL lanes fetch one sample's 8 corner rows as 16-byte
+        // (bf16 x 8) loads, kGPS samples per step; each lane stages 8 interpolated channels
+        using GL = GatherLanes<S, kDeg>;
+        constexpr int kGL = GL::kLanes, kGPS = GL::kPerStep;
+        const int q8 = lane % kGL;
+#pragma unroll kGatherUnroll
+        for (int st = 0; st < kGL; ++st) {
+            const int j = st * kGPS + lane / kGL;
+            const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
+            const float gx = __shfl_sync(kFull, s.wx, j), gy = __shfl_sync(kFull, s.wy, j),
+                        gz = __shfl_sync(kFull, s.wz, j);
+            const bool gok = __shfl_sync(kFull, s.valid, j);
+            float v[8];
+            if (gok) {
+                const uint4 v000 = Store<S>::oct(p.data, vb, q8, kC), v001 = Store<S>::oct(p.data, vb + 1, q8, kC);
+                const uint4 v010 = Store<S>::oct(p.data, vb + sy, q8, kC),
+                            v011 = Store<S>::oct(p.data, vb + sy + 1, q8, kC);
+                const uint4 v100 = Store<S>::oct(p.data, vb + sz, q8, kC),
+                            v101 = Store<S>::oct(p.data, vb + sz + 1, q8, kC);
+                const uint4 v110 = Store<S>::oct(p.data, vb + sz + sy, q8, kC),
+                            v111 = Store<S>::oct(p.data, vb + sz + sy + 1, q8, kC);
+                float x00[8], x01[8], x10[8], x11[8];
+                lerp_bf8(v000, v001, gx, x00);
+                lerp_bf8(v010, v011, gx, x01);
+                lerp_bf8(v100, v101, gx, x10);
+                lerp_bf8(v110, v111, gx, x11);
+#pragma unroll
+                for (int t = 0; t < 8; ++t)
+                    v[t] = lerp_ref(lerp_ref(x00[t], x01[t], gy), lerp_ref(x10[t], x11[t], gy), gz);
+            } else {
+#pragma unroll
+                for (int t = 0; t < 8; ++t) v[t] = 0.0f;
+            }
+            const float4 lo = make_float4(v[0], v[1], v[2], v[3]), hi = make_float4(v[4], v[5], v[6], v[7]);
+            // with 8 lanes per row (64 channels) lanes 4..7 store their halves in the other
+            // order, so each 8-lane phase of a store covers 32 distinct banks
+            const bool swap = (q8 & 4) != 0;
+            st4(tile + j * kRow + 8 * q8 + (swap ? 4 : 0), swap ? hi : lo);
+            st4(tile + j * kRow + 8 * q8 + (swap ? 0 : 4), swap ? lo : hi);
+            if (to_slot) {
+                const uint64_t pol = evict_last_policy();
+                st4_keep(to_slot + j * kC + 8 * q8, lo, pol);
+                st4_keep(to_slot + j * kC + 8 * q8 + 4, hi, pol);
+            }
+        }
+    } else {
+    // gather: groups of kL lanes fetch one sample's 8 corner rows, kPS samples per step
 #pragma unroll kGatherUnroll
     for (int st = 0; st < kL; ++st) {
         const int j = st * kPS + lane / kL;
@@ -402,6 +470,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
         }
         st4(tile + j * kRow + 4 * q, v);
         if (to_slot) st4_keep(to_slot + j * kC + 4 * q, v, evict_last_policy());
+    }
     }
     __syncwarp();
     if (s.valid) {
