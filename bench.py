@@ -386,7 +386,7 @@ def run_ours(args, cfg, device, ws, rank):
     if ws == 1 and args.workload == "plain256" and not args.no_proposal:
         del scene, batches
         torch.cuda.empty_cache()
-        out["proposal"] = proposal_comparison(PROPOSAL_STEPS)
+        out["proposal"] = proposal_comparison(PROPOSAL_STEPS, args.proposal_warmup)
     return out
 
 
@@ -440,12 +440,12 @@ def full_step_parts(args, cfg, batches, sdf, data, sdf_k, data_k, sg, dg, mode, 
 
 # ----------------------------------------------------------------------------- proposal path
 
-def proposal_comparison(steps: int):
+def proposal_comparison(steps: int, warmup_frac: float = 0.2):
     """Training at 256^3 from the same initial model on the same ray pool: the uniform march
     (256 samples/ray, 65536 rays/step) and the proposal path (64 coarse MLP points + 32 fine
     samples/ray, network trained online every step; twice the rays per step, which costs
-    about the render time of one plain step; the first 20% of its steps use the uniform march
-    while the network learns).  rays/s is device time of the forward + backward part of the
+    about the render time of one plain step; the first ``warmup_frac`` of its steps use the
+    uniform march while the network learns).  rays/s is device time of the forward + backward part of the
     steps (for the proposal: coarse MLP, sampler, online network update and the fused train
     launch); PSNR is on 65536 held-out rays rendered by the uniform march."""
     from qsdvr_b200 import train
@@ -455,7 +455,7 @@ def proposal_comparison(steps: int):
     data = train.build(a.reso, a.views, a.size, 1111.1 * a.size / 800, 4.03, a.interval, a.k, a.seed,
                        torch.device("cuda", torch.cuda.current_device()))
     plain = train.run(a, data, quiet=True)
-    a.proposal, a.rays, a.proposal_mix, a.proposal_warmup = True, 2 * a.rays, 0.05, steps // 5
+    a.proposal, a.rays, a.proposal_mix, a.proposal_warmup = True, 2 * a.rays, 0.05, int(round(steps * warmup_frac))
     prop = train.run(a, data, quiet=True)
     del data
     torch.cuda.empty_cache()
@@ -739,6 +739,8 @@ def main():
     ap.add_argument("--cpu-rays", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-proposal", action="store_true", help="skip the proposal-path comparison")
+    ap.add_argument("--proposal-warmup", type=float, default=0.2,
+                    help="fraction of the proposal run's steps trained with the uniform march first")
     ap.add_argument("--views", type=int, default=None, help="override the number of camera views (ray pool size)")
     args = ap.parse_args()
     if args.warmup < 3:

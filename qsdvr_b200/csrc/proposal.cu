@@ -455,68 +455,104 @@ __global__ void __launch_bounds__(128, 5) mlp_infer_kernel(const float4 *__restr
 }
 
 // ---- coarse-to-fine sampling ---------------------------------------------------------------
-// One warp per ray: coarse opacity a_j = 1 - exp(-s_j L/64), weights T_j a_j, a pdf mixed with
-// the fraction uniform_mix of uniform, and the 33 fine SDF positions at the CDF quantiles k/32
-// (t_0 = 0, t_32 = L).
+// One warp per kSampleRays rays, processed in lockstep so that their memory and shuffle
+// latencies overlap: coarse opacity a_j = 1 - exp(-s_j L/64), weights T_j a_j, a pdf mixed
+// with the fraction uniform_mix of uniform, and the 33 fine SDF positions at the CDF
+// quantiles k/32 (t_0 = 0, t_32 = L).
+constexpr int kSampleRays = 4;
+
 __global__ void __launch_bounds__(256) proposal_sample_kernel(const qsdvr_ray_info *__restrict__ rays,
                                                               uint32_t nrays, float interval, float uniform_mix,
                                                               const float *__restrict__ dens,
                                                               float *__restrict__ tlist) {
-    __shared__ float cdf_s[8][65];
+    constexpr int kR = kSampleRays;
+    __shared__ float cdf_s[8][kR][65];
     const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t r = blockIdx.x * 8 + w;
-    if (r >= nrays) return;
-    const uint32_t ns = rays[r].sdf_count;
-    const float L = ns > 1 ? (float)(ns - 1) * interval : 0.0f;
-    const float delta = L / 64.0f;
-    float *cdf = cdf_s[w];
-    // two coarse bins per lane: j = 2 lane, 2 lane + 1
-    const float s0 = dens[64ull * r + 2 * lane], s1 = dens[64ull * r + 2 * lane + 1];
-    const float t0 = expf(-fmaxf(s0, 0.0f) * delta), t1 = expf(-fmaxf(s1, 0.0f) * delta);  // 1 - alpha
-    float incl = t0 * t1;
+    const uint32_t r0 = (blockIdx.x * 8 + w) * kR;
+    if (r0 >= nrays) return;
+    float L[kR], delta[kR], t0[kR], t1[kR];
+#pragma unroll
+    for (int q = 0; q < kR; ++q) {
+        const uint32_t r = r0 + q;
+        const bool have = r < nrays;  // warp-uniform
+        const uint32_t ns = have ? rays[r].sdf_count : 0u;
+        L[q] = ns > 1 ? (float)(ns - 1) * interval : 0.0f;
+        delta[q] = L[q] / 64.0f;
+        // two coarse bins per lane: j = 2 lane, 2 lane + 1
+        const float s0 = have ? dens[64ull * r + 2 * lane] : 0.0f, s1 = have ? dens[64ull * r + 2 * lane + 1] : 0.0f;
+        t0[q] = expf(-fmaxf(s0, 0.0f) * delta[q]);  // 1 - alpha
+        t1[q] = expf(-fmaxf(s1, 0.0f) * delta[q]);
+    }
+    float incl[kR];
+#pragma unroll
+    for (int q = 0; q < kR; ++q) incl[q] = t0[q] * t1[q];
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const float v = __shfl_up_sync(kFull, incl, o);
-        if ((int)lane >= o) incl *= v;
-    }
-    float T = __shfl_up_sync(kFull, incl, 1);
-    if (lane == 0) T = 1.0f;
-    const float w0 = T * (1.0f - t0), w1 = T * t0 * (1.0f - t1);
-    float sum = w0 + w1;
 #pragma unroll
-    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
-    const float mix = uniform_mix / 64.0f, keep = 1.0f - uniform_mix;
-    const float p0 = sum > 0.0f ? keep * w0 / sum + mix : 1.0f / 64.0f;
-    const float p1 = sum > 0.0f ? keep * w1 / sum + mix : 1.0f / 64.0f;
-    float c = p0 + p1;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const float v = __shfl_up_sync(kFull, c, o);
-        if ((int)lane >= o) c += v;
-    }
-    const float total = __shfl_sync(kFull, c, 31);
-    cdf[2 * lane + 1] = (c - p1) / total;
-    cdf[2 * lane + 2] = c / total;
-    if (lane == 0) cdf[0] = 0.0f;
-    __syncwarp();
-    for (uint32_t k = lane; k <= 32; k += 32) {
-        float tk;
-        if (k == 0) {
-            tk = 0.0f;
-        } else if (k == 32) {
-            tk = L;
-        } else {
-            const float q = (float)k / 32.0f;
-            int lo = 0, hi = 64;  // cdf[lo] <= q < cdf[hi]
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (cdf[mid] <= q) lo = mid; else hi = mid;
-            }
-            const float span = cdf[lo + 1] - cdf[lo];
-            const float frac = span > 0.0f ? (q - cdf[lo]) / span : 0.5f;
-            tk = fminf(((float)lo + fminf(fmaxf(frac, 0.0f), 1.0f)) * delta, L);
+        for (int q = 0; q < kR; ++q) {
+            const float v = __shfl_up_sync(kFull, incl[q], o);
+            if ((int)lane >= o) incl[q] *= v;
         }
-        tlist[33ull * r + k] = tk;
+    }
+    float w0[kR], w1[kR], sum[kR];
+#pragma unroll
+    for (int q = 0; q < kR; ++q) {
+        float T = __shfl_up_sync(kFull, incl[q], 1);
+        if (lane == 0) T = 1.0f;
+        w0[q] = T * (1.0f - t0[q]);
+        w1[q] = T * t0[q] * (1.0f - t1[q]);
+        sum[q] = w0[q] + w1[q];
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+#pragma unroll
+        for (int q = 0; q < kR; ++q) sum[q] += __shfl_xor_sync(kFull, sum[q], o);
+    }
+    const float mix = uniform_mix / 64.0f, keep = 1.0f - uniform_mix;
+    float p1[kR], c[kR];
+#pragma unroll
+    for (int q = 0; q < kR; ++q) {
+        const float p0 = sum[q] > 0.0f ? keep * w0[q] / sum[q] + mix : 1.0f / 64.0f;
+        p1[q] = sum[q] > 0.0f ? keep * w1[q] / sum[q] + mix : 1.0f / 64.0f;
+        c[q] = p0 + p1[q];
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+        for (int q = 0; q < kR; ++q) {
+            const float v = __shfl_up_sync(kFull, c[q], o);
+            if ((int)lane >= o) c[q] += v;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kR; ++q) {
+        const float total = __shfl_sync(kFull, c[q], 31);
+        float *cdf = cdf_s[w][q];
+        cdf[2 * lane + 1] = (c[q] - p1[q]) / total;
+        cdf[2 * lane + 2] = c[q] / total;
+        if (lane == 0) cdf[0] = 0.0f;
+    }
+    __syncwarp();
+    // quantile k = lane (k = 0 is t = 0) and, on lane 0, k = 32 (t = L); the bisection
+    // cdf[lo] <= k/32 < cdf[lo + 1] over 64 bins takes exactly 6 halvings
+#pragma unroll
+    for (int q = 0; q < kR; ++q) {
+        const uint32_t r = r0 + q;
+        if (r >= nrays) break;
+        const float *cdf = cdf_s[w][q];
+        float tk = 0.0f;
+        if (lane > 0) {
+            const float qk = (float)lane / 32.0f;
+            int lo = 0;
+#pragma unroll
+            for (int step = 32; step >= 1; step >>= 1)
+                if (cdf[lo + step] <= qk) lo += step;
+            const float span = cdf[lo + 1] - cdf[lo];
+            const float frac = span > 0.0f ? (qk - cdf[lo]) / span : 0.5f;
+            tk = fminf(((float)lo + fminf(fmaxf(frac, 0.0f), 1.0f)) * delta[q], L[q]);
+        }
+        tlist[33ull * r + lane] = tk;
+        if (lane == 0) tlist[33ull * r + 32] = L[q];
     }
 }
 
@@ -715,8 +751,9 @@ extern "C" int qsdvr_proposal_sample(const qsdvr_ray_info *rays, uint32_t ray_co
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_proposal_sample: null pointer");
     if (!(uniform_mix > 0.0f && uniform_mix <= 1.0f))
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_proposal_sample: uniform_mix must be in (0, 1]");
-    proposal_sample_kernel<<<grid_for(ray_count, 8), 256, 0, stream>>>(rays, ray_count, interval, uniform_mix,
-                                                                       coarse_density, tlist);
+    proposal_sample_kernel<<<grid_for(ray_count, 8 * kSampleRays), 256, 0, stream>>>(rays, ray_count, interval,
+                                                                                     uniform_mix, coarse_density,
+                                                                                     tlist);
     return check_launch("qsdvr_proposal_sample");
 }
 
