@@ -7,6 +7,10 @@ tables to the host after RayCut and back on every call).
 """
 from __future__ import annotations
 
+import struct
+import zlib
+
+import numpy as np
 import torch
 
 from . import qsdvr
@@ -49,6 +53,39 @@ class Camera:
         direction = torch.zeros((P, 3), dtype=torch.float32, device=dev)
         qsdvr.RayCut(self.args, mask, rays, origin, direction, self.interval)
         m = mask.reshape(-1)[:P].to(dev, torch.bool)
+        self.mask = m
         self.rayList = rays[m].contiguous()
         self.originList = origin[m].contiguous()
         self.dirList = direction[m].contiguous()
+
+    def whole_image(self, colors: torch.Tensor) -> torch.Tensor:
+        """datasets/nerf_dataset.py:92-96 (get_whole_image): the masked rays' colours [N, 3]
+        scattered into a [height, width, 3] frame, zero where the mask is off (on the
+        colours' device)."""
+        a = self.args
+        m = self.mask.to(colors.device)
+        if colors.shape != (int(m.sum()), 3):
+            raise ValueError(f"colors must be [{int(m.sum())}, 3], got {tuple(colors.shape)}")
+        img = torch.zeros((a.height * a.width, 3), dtype=colors.dtype, device=colors.device)
+        img[m] = colors
+        return img.reshape(a.height, a.width, 3)
+
+
+def save_png(path: str, image) -> None:
+    """Write an [H, W, 3] image with values in [0, 1] as an 8-bit RGB PNG, as test.py:41-44
+    does with imageio ((img * 255).clip(0, 255) as uint8), using only the standard library."""
+    img = image.detach().cpu().numpy() if isinstance(image, torch.Tensor) else np.asarray(image)
+    if img.ndim != 3 or img.shape[2] != 3:
+        raise ValueError("image must be [H, W, 3]")
+    px = (img * 255).clip(0, 255).astype(np.uint8)
+    h, w = px.shape[:2]
+    raw = b"".join(b"\x00" + px[y].tobytes() for y in range(h))  # filter type 0 per row
+
+    def chunk(tag: bytes, body: bytes) -> bytes:
+        return struct.pack(">I", len(body)) + tag + body + struct.pack(">I", zlib.crc32(tag + body) & 0xFFFFFFFF)
+
+    with open(path, "wb") as f:
+        f.write(b"\x89PNG\r\n\x1a\n")
+        f.write(chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0)))
+        f.write(chunk(b"IDAT", zlib.compress(raw, 6)))
+        f.write(chunk(b"IEND", b""))

@@ -86,3 +86,44 @@ def test_camera_args_fields():
     a.rotation = [1, 2]
     with pytest.raises(ValueError):
         a.to_c()
+
+
+def test_whole_image_and_png(tmp_path):
+    """Image assembly (datasets/nerf_dataset.py:92-96) and the PNG writer, on the CPU: the
+    masked rays' colours land at their pixels, zeros elsewhere; the PNG decodes back to the
+    same 8-bit pixels."""
+    import struct
+    import zlib
+
+    import numpy as np
+    import torch
+
+    from qsdvr_b200.camera import Camera, save_png
+    from qsdvr_b200.qsdvr import CameraArgs
+
+    a = CameraArgs()
+    a.width, a.height = 5, 3
+    cam = Camera(a, device="cpu")
+    mask = torch.zeros(15, dtype=torch.bool)
+    mask[[0, 4, 7, 14]] = True
+    cam.mask = mask
+    colors = torch.tensor([[0.1, 0.2, 0.3], [1.0, 0.0, 0.5], [0.25, 0.75, 1.5], [-0.2, 0.6, 0.9]])
+    img = cam.whole_image(colors)
+    assert img.shape == (3, 5, 3)
+    flat = img.reshape(-1, 3)
+    assert torch.equal(flat[mask], colors) and not flat[~mask].any()
+    with pytest.raises(ValueError):
+        cam.whole_image(colors[:3])
+    path = tmp_path / "frame.png"
+    save_png(str(path), img)
+    data = path.read_bytes()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    w, h = struct.unpack(">II", data[16:24])
+    assert (w, h) == (5, 3)
+    i = data.index(b"IDAT")
+    n = struct.unpack(">I", data[i - 4:i])[0]
+    raw = zlib.decompress(data[i + 4:i + 4 + n])
+    rows = np.frombuffer(raw, np.uint8).reshape(3, 1 + 5 * 3)
+    assert not rows[:, 0].any()
+    want = (img.numpy() * 255).clip(0, 255).astype(np.uint8).reshape(3, 15)
+    assert np.array_equal(rows[:, 1:], want)
