@@ -172,7 +172,8 @@ def test_autograd_function_matches_train_kernel(fz):
     col, ls = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, model.sdfGrid.detach(),
                               model.renderData.detach(), R, interval, k, sg, dg, mode="fixed")
     assert (col - img.detach()).abs().max().item() < 1e-6
-    assert abs(ls.item() / (3 * col.shape[0]) - loss.item()) < 1e-6
+    # the kernel's loss is summed by float atomics in launch order: within n * 2^-24 of the total
+    assert abs(ls.item() / (3 * col.shape[0]) - loss.item()) <= col.shape[0] * 2.0 ** -24 * max(1e-6, loss.item())
     assert rel_err(model.sdfGrid.grad.cpu(), sg.cpu()) < 1e-6
     assert rel_err(model.renderData.grad.cpu(), dg.cpu()) < 1e-6
 
@@ -213,7 +214,8 @@ def test_persistent_stash_path_matches_one_ray_per_block(fz, mode):
         out.append((col, loss, sg, dg))
     (c0, l0, s0, d0), (c1, l1, s1, d1) = out
     assert (c0 - c1).abs().max().item() < 1e-6
-    assert abs(l0.item() - l1.item()) < 1e-5 * max(1.0, l0.item())
+    # losses summed by float atomics in launch order: within n * 2^-24 of the total
+    assert abs(l0.item() - l1.item()) <= c0.shape[0] * 2.0 ** -24 * max(1.0, l0.item())
     assert rel_err(s1.cpu(), s0.cpu()) < 1e-5 and rel_err(d1.cpu(), d0.cpu()) < 1e-5
 
 

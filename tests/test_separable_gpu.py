@@ -87,7 +87,10 @@ def test_separable_gradients_match_dense_path(qs, mode):
     c1, l1 = fused.render_train(target, *args, None, data, R, interval, k, tg, dg2, mode, sdf_layers=tables)
     got = fused.separable_grad(tg)
     assert torch.equal(c0, c1)
-    assert abs(l0.item() - l1.item()) <= 1e-6 * max(1.0, l0.item())
+    # the same colours, their squared errors summed by float atomics in launch order: the two
+    # sums differ by at most the float32 summation bound n * 2^-24 of the total
+    n = cam.rayList.shape[0]
+    assert abs(l0.item() - l1.item()) <= n * 2.0 ** -24 * max(1.0, l0.item())
     assert rel_err(dg2.cpu(), dg.cpu()) < 1e-6
     for g, w in zip(got, want):
         assert rel_err(g.cpu(), w.cpu()) < 1e-5
