@@ -715,7 +715,8 @@ def run_reference(args, cfg):
         _cpu_step(grid7, data_cpu, b, cfg["R"], cfg["interval"])
     dt = time.perf_counter() - t0
     value = args.cpu_rays * args.steps / dt
-    line = {"metric": METRIC, "impl": "reference", "value": round(value, 2), "unit": "rays/s", "n_gpus": 0,
+    # n_gpus mirrors the launch (--gpus N); the timed work runs on rank 0's host cores
+    line = {"metric": METRIC, "impl": "reference", "value": round(value, 2), "unit": "rays/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (same seeded scene and batch as the GPU arm)",
