@@ -58,6 +58,10 @@ WORKLOADS = {
                    storage="f32", online_steps=200),
     "proposal384": dict(R=384, rays=65536, views=200, size=800, focal=1111.1, radius=4.03, interval=4.0 / 512,
                         storage="bf16", sh=3, train_steps=200, heldout=4),
+    # training comparison at 512 samples/ray (the learned proposal form's uniform march) on the
+    # 256^3 scene: proposal path against the uniform march, rays/s and held-out PSNR
+    "train512": dict(R=256, rays=65536, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 512,
+                     storage="f32"),
 }
 PROPOSAL_STEPS = 300  # training steps per method in the default line's proposal comparison
 
@@ -440,9 +444,9 @@ def full_step_parts(args, cfg, batches, sdf, data, sdf_k, data_k, sg, dg, mode, 
 
 # ----------------------------------------------------------------------------- proposal path
 
-def proposal_comparison(steps: int, warmup_frac: float = 0.2):
+def proposal_comparison(steps: int, warmup_frac: float = 0.2, interval: float = 4.0 / 256):
     """Training at 256^3 from the same initial model on the same ray pool: the uniform march
-    (256 samples/ray, 65536 rays/step) and the proposal path (64 coarse MLP points + 32 fine
+    (4 / interval samples/ray, 65536 rays/step) and the proposal path (64 coarse MLP points + 32 fine
     samples/ray, network trained online every step; twice the rays per step, which costs
     about the render time of one plain step; the first ``warmup_frac`` of its steps use the
     uniform march while the network learns).  rays/s is device time of the forward + backward part of the
@@ -451,7 +455,7 @@ def proposal_comparison(steps: int, warmup_frac: float = 0.2):
     from qsdvr_b200 import train
 
     a = train.parser().parse_args([])
-    a.steps, a.log_every = steps, 10 ** 9
+    a.steps, a.log_every, a.interval = steps, 10 ** 9, interval
     data = train.build(a.reso, a.views, a.size, 1111.1 * a.size / 800, 4.03, a.interval, a.k, a.seed,
                        torch.device("cuda", torch.cuda.current_device()))
     plain = train.run(a, data, quiet=True)
@@ -553,6 +557,22 @@ def run_mlp_kernels(args, cfg, device):
                      "frac": round(tflops / peak[0], 4), "traffic": None, "kernel": "mlp_infer_kernel",
                      "flops_per_point": MLP_FLOPS_PER_POINT, "peak_kind": peak[1]},
         "kernels": side, "clocks": clk.summary(),
+    }
+
+
+def run_train512(args, cfg, device):
+    """The default line's proposal comparison with the uniform march at 512 samples/ray (the
+    learned proposal form's reference march) on the 256^3 scene."""
+    cmp = proposal_comparison(PROPOSAL_STEPS, args.proposal_warmup, cfg["interval"])
+    return {
+        "metric": "train rays/s fwd+bwd @256^3: proposal (64 coarse + 32 fine) vs 512-sample uniform march",
+        "value": cmp["train_rays_per_s"], "unit": "rays/s", "n_gpus": 1, "steps": PROPOSAL_STEPS,
+        "warmup": int(round(PROPOSAL_STEPS * args.proposal_warmup)), "ms_per_step": cmp["render_ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded procedural scene; model trained from a sphere init)",
+        "config": {"workload": "train512: " + cmp["workload"] + ", interval 4/512",
+                   "global_batch": 2 * cfg["rays"], "parallelism": "replicas x1"},
+        "gpu_launches": None, "proposal": cmp,
     }
 
 
@@ -762,10 +782,11 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=device)
     try:
-        if args.workload in ("proposal384", "mlp256"):
+        if args.workload in ("proposal384", "mlp256", "train512"):
             if ws > 1:
                 raise SystemExit(f"{args.workload} is a single-GPU workload")
-            fn = run_proposal_frames if args.workload == "proposal384" else run_mlp_kernels
+            fn = {"proposal384": run_proposal_frames, "mlp256": run_mlp_kernels,
+                  "train512": run_train512}[args.workload]
             print(json.dumps(fn(args, cfg, device)))
             return
         out = run_ours(args, cfg, device, ws, rank)

@@ -14,6 +14,10 @@ MLP evaluations place them) instead of the uniform march (after ``--proposal-war
 with it).  The network is trained online every step on the per-sample alphas of a
 uniform-march forward over part of the batch.
 Held-out PSNR is always measured with the uniform march.
+
+``--save PATH`` writes a checkpoint (checkpoint.py) at the end and every ``--save-every``
+steps; ``--resume PATH`` continues a run from one, with the same ray batches as the run that
+was not interrupted.
 """
 from __future__ import annotations
 
@@ -24,7 +28,7 @@ import time
 
 import torch
 
-from . import fused, scenes
+from . import checkpoint, fused, scenes
 from .camera import Camera
 from .optim import FusedGridAdam
 
@@ -74,6 +78,9 @@ def parser():
     ap.add_argument("--proposal-warmup", type=int, default=0,
                     help="steps trained with the uniform march (network trained online) before the proposal")
     ap.add_argument("--log-every", type=int, default=100)
+    ap.add_argument("--save", default=None, help="checkpoint path written at the end (and every --save-every)")
+    ap.add_argument("--save-every", type=int, default=0)
+    ap.add_argument("--resume", default=None, help="checkpoint to continue from (steps counts the total)")
     ap.add_argument("--seed", type=int, default=0)
     return ap
 
@@ -102,6 +109,9 @@ def run(a, data=None, quiet=False, return_state=False):
     model.sdfGrid.grad = torch.zeros_like(model.sdfGrid)
     model.renderData.grad = torch.zeros_like(model.renderData)
     net = ProposalNet(dev, seed=a.seed, lr=a.proposal_lr) if (a.proposal or a.online_proposal) else None
+    first = 1
+    if getattr(a, "resume", None):
+        first = checkpoint.load(a.resume, model, opt, net, gen) + 1
     loss = torch.zeros(1, dtype=torch.float32, device=dev)
     log = []
 
@@ -117,16 +127,17 @@ def run(a, data=None, quiet=False, return_state=False):
         return out
 
     start = evaluate()
+    steps = range(first, a.steps + 1)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+           torch.cuda.Event(enable_timing=True)) for _ in steps]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for step in range(1, a.steps + 1):
+    for step in steps:
         idx = torch.randint(0, total, (a.rays,), generator=gen, device=dev)
         r, o, d, tg = rays[idx], origin[idx], direction[idx], target[idx]
         sg, dg = model.grids()
         sg, dg = sg.detach(), dg.detach()
-        e0, e1, e2 = ev[step - 1]
+        e0, e1, e2 = ev[step - first]
         e0.record()
         loss.zero_()
         tlist = None
@@ -146,20 +157,24 @@ def run(a, data=None, quiet=False, return_state=False):
             mse = float(loss) / (3 * a.rays)
             log.append({"step": step, "train_mse": mse, "elapsed_s": round(time.perf_counter() - t0, 3)})
             print(json.dumps(log[-1]), flush=True)
+        if getattr(a, "save", None) and ((a.save_every and step % a.save_every == 0) or step == a.steps):
+            checkpoint.save(a.save, model, opt, net, step, gen)
     torch.cuda.synchronize()
     elapsed = time.perf_counter() - t0
     render_ms = sum(e0.elapsed_time(e1) for e0, e1, _ in ev)
     opt_ms = sum(e1.elapsed_time(e2) for _, e1, e2 in ev)
-    warm = a.proposal_warmup if a.proposal else 0
+    warm = max(0, (a.proposal_warmup if a.proposal else 0) - (first - 1))
     steady = [e0.elapsed_time(e1) for e0, e1, _ in ev[warm:]]
     end = evaluate()
-    out = {"reso": R, "steps": a.steps, "rays_per_step": a.rays, "lr": a.lr, "storage": a.storage, "mode": a.mode,
+    ran = len(steps)  # steps run in this call (all of them unless resumed)
+    out = {"reso": R, "steps": a.steps, "first_step": first, "rays_per_step": a.rays, "lr": a.lr, "storage": a.storage, "mode": a.mode,
            "sh_degree": a.sh, "k": a.k,
            "method": "proposal 64 coarse + 32 fine" if a.proposal else
                      "uniform march" + (" + online proposal network" if net else ""),
-           "ms_per_step": round(1e3 * elapsed / a.steps, 3), "train_rays_per_s": round(a.steps * a.rays / elapsed),
+           "ms_per_step": round(1e3 * elapsed / max(ran, 1), 3),
+           "train_rays_per_s": round(ran * a.rays / elapsed) if ran else None,
            "render_ms": round(render_ms, 3), "optimizer_ms": round(opt_ms, 3),
-           "render_rays_per_s": round(a.steps * a.rays / (render_ms / 1e3)),
+           "render_rays_per_s": round(ran * a.rays / (render_ms / 1e3)) if ran else None,
            "steady_render_rays_per_s": round(len(steady) * a.rays / (sum(steady) / 1e3)) if steady else None,
            "heldout_psnr_start": round(psnr(start["uniform"]), 3), "heldout_psnr_end": round(psnr(end["uniform"]), 3),
            "peak_memory_gb": round(torch.cuda.max_memory_allocated(dev) / 1e9, 3),
