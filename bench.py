@@ -608,7 +608,7 @@ def run_proposal_frames(args, cfg, device):
     for cam in scenes.hemisphere_cameras(cfg["heldout"], cfg["radius"], size, size, cfg["focal"], 2.0, 6.0,
                                          seed=a.seed + 99):
         c = Camera(cam, interval, R, device=device)
-        c.GenerateRayPoints(torch.ones(size * size, dtype=torch.bool))
+        c.GenerateRayPoints(torch.ones(size * size, dtype=torch.bool), order=args.ray_order)
         gt = fused.render_forward(c.rayList, c.originList, c.dirList, gt_sdf, gt_data, R, interval, a.k, "fixed")
         frames.append((c.rayList, c.originList, c.dirList, gt))
     del gt_sdf, gt_data
@@ -652,6 +652,7 @@ def run_proposal_frames(args, cfg, device):
                                f"({a.rays} rays/step, uniform 512 march, proposal network trained online), "
                                f"{cfg['heldout']} held-out {size}^2 frames, k={a.k}",
                    "global_batch": pixels, "step": "one full frame (all pixels, hit or not)",
+                   "ray_order": args.ray_order,
                    "l2": "grids 8.2 GB, larger than L2; no flush", "parallelism": "replicas x1"},
         "plain_value": round(plain, 1), "speedup": round(value / plain, 3),
         "psnr_uniform512": round(out["uniform"]["psnr"], 3), "psnr_proposal": round(out["proposal"]["psnr"], 3),
@@ -763,6 +764,8 @@ def main():
     ap.add_argument("--proposal-warmup", type=float, default=0.2,
                     help="fraction of the proposal run's steps trained with the uniform march first")
     ap.add_argument("--views", type=int, default=None, help="override the number of camera views (ray pool size)")
+    ap.add_argument("--ray-order", default="pixels", choices=["pixels", "tiles"],
+                    help="order of a full frame's rays (proposal384): row-major pixels or 8x8 tiles")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

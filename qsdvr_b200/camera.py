@@ -44,8 +44,15 @@ class Camera:
                                 self.reso)
         return d
 
-    def GenerateRayPoints(self, mask: torch.Tensor):
-        """datasets/utils.py:42-56: RayCut over all pixels, then keep the masked rays."""
+    def GenerateRayPoints(self, mask: torch.Tensor, order: str = "pixels", tile: int = 8):
+        """datasets/utils.py:42-56: RayCut over all pixels, then keep the masked rays.
+
+        ``order="pixels"`` keeps the reference's row-major pixel order.  ``order="tiles"``
+        lists the rays tile by tile (``tile`` x ``tile`` pixels, tiles and the pixels inside
+        them row-major), so that rays adjacent in the list are adjacent on the image; each
+        ray keeps its RayCut record, and ``pixel_index`` maps the list back to pixels."""
+        if order not in ("pixels", "tiles"):
+            raise ValueError(f"order must be 'pixels' or 'tiles', got {order!r}")
         dev = self.device
         P = self.args.pixelCount
         rays = torch.zeros((P, 4), dtype=torch.int32, device=dev)
@@ -54,21 +61,34 @@ class Camera:
         qsdvr.RayCut(self.args, mask, rays, origin, direction, self.interval)
         m = mask.reshape(-1)[:P].to(dev, torch.bool)
         self.mask = m
-        self.rayList = rays[m].contiguous()
-        self.originList = origin[m].contiguous()
-        self.dirList = direction[m].contiguous()
+        pix = torch.nonzero(m).reshape(-1)
+        if order == "tiles":
+            pix = tile_order(pix, self.args.width, tile)
+        self.pixel_index = pix
+        self.rayList = rays[pix].contiguous()
+        self.originList = origin[pix].contiguous()
+        self.dirList = direction[pix].contiguous()
 
     def whole_image(self, colors: torch.Tensor) -> torch.Tensor:
-        """datasets/nerf_dataset.py:92-96 (get_whole_image): the masked rays' colours [N, 3]
-        scattered into a [height, width, 3] frame, zero where the mask is off (on the
-        colours' device)."""
+        """datasets/nerf_dataset.py:92-96 (get_whole_image): the rays' colours [N, 3] (in the
+        order of rayList) scattered into a [height, width, 3] frame, zero where the mask is
+        off (on the colours' device)."""
         a = self.args
-        m = self.mask.to(colors.device)
-        if colors.shape != (int(m.sum()), 3):
-            raise ValueError(f"colors must be [{int(m.sum())}, 3], got {tuple(colors.shape)}")
+        pix = self.pixel_index.to(colors.device)
+        if colors.shape != (pix.numel(), 3):
+            raise ValueError(f"colors must be [{pix.numel()}, 3], got {tuple(colors.shape)}")
         img = torch.zeros((a.height * a.width, 3), dtype=colors.dtype, device=colors.device)
-        img[m] = colors
+        img[pix] = colors
         return img.reshape(a.height, a.width, 3)
+
+
+def tile_order(pixels: torch.Tensor, width: int, tile: int = 8) -> torch.Tensor:
+    """``pixels`` (row-major indices of an image ``width`` wide) listed tile by tile: tiles of
+    ``tile`` x ``tile`` pixels in row-major order, the pixels of a tile row-major inside it."""
+    y, x = pixels // width, pixels % width
+    ntx = (width + tile - 1) // tile
+    key = ((y // tile) * ntx + x // tile) * (tile * tile) + (y % tile) * tile + (x % tile)
+    return pixels[torch.argsort(key)]
 
 
 def save_png(path: str, image) -> None:

@@ -107,6 +107,7 @@ def test_whole_image_and_png(tmp_path):
     mask = torch.zeros(15, dtype=torch.bool)
     mask[[0, 4, 7, 14]] = True
     cam.mask = mask
+    cam.pixel_index = torch.nonzero(mask).reshape(-1)
     colors = torch.tensor([[0.1, 0.2, 0.3], [1.0, 0.0, 0.5], [0.25, 0.75, 1.5], [-0.2, 0.6, 0.9]])
     img = cam.whole_image(colors)
     assert img.shape == (3, 5, 3)
@@ -127,3 +128,21 @@ def test_whole_image_and_png(tmp_path):
     assert not rows[:, 0].any()
     want = (img.numpy() * 255).clip(0, 255).astype(np.uint8).reshape(3, 15)
     assert np.array_equal(rows[:, 1:], want)
+
+
+def test_tile_order():
+    """Rays listed tile by tile: the first 64 of a 20 x 12 image are its top-left 8 x 8 tile,
+    row-major; partial edge tiles follow in row-major tile order; nothing is lost."""
+    import torch
+
+    from qsdvr_b200.camera import tile_order
+
+    w, h = 20, 12
+    pix = torch.arange(w * h)
+    out = tile_order(pix, w, 8)
+    assert torch.equal(out.sort().values, pix)
+    assert torch.equal(out[:64], torch.tensor([y * w + x for y in range(8) for x in range(8)]))
+    assert torch.equal(out[64:128], torch.tensor([y * w + x for y in range(8) for x in range(8, 16)]))
+    assert torch.equal(out[128:160], torch.tensor([y * w + x for y in range(8) for x in range(16, 20)]))
+    masked = pix[pix % 3 == 0]
+    assert torch.equal(tile_order(masked, w, 8).sort().values, masked)
