@@ -192,6 +192,50 @@ __device__ __forceinline__ uint64_t forward_tile(uint8_t *xs, uint8_t *hs, uint8
     return mask;
 }
 
+// Inference forward of one tile with X and H1 in the same buffer (X is dead once layer 1
+// has run) and the TMEM results read in halves of 32 columns, so that a CTA needs ~35 KB of
+// shared memory and at most 80 registers a thread: six CTAs per SM.  Returns the head's
+// pre-activation w3 . relu(z2) + b3.
+__device__ __forceinline__ float infer_tile(uint8_t *buf, uint8_t *w1s, uint8_t *w2s, uint32_t d1, Sync &sync,
+                                            const float *w3, float b3) {
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+    constexpr uint32_t i1 = tc::idesc_bf16(128, 64, false, false);
+    handoff();
+    if (t == 0) {
+        for (int s = 0; s < 2; ++s)
+            tc::mma_bf16(d1, tc::smem_desc(tc::smem_addr(buf) + 256 * s, 128, kSpX),
+                         tc::smem_desc(tc::smem_addr(w1s) + 256 * s, 128, kSoW1), i1, s > 0);
+    }
+    sync.complete();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        float v[32];
+        tc::tmem_ld32(tc::tmem_at(d1, 32 * warp, 32 * h), v);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) store_relu_row8(buf, t, 4 * h + g, kSpH, v + 8 * g);
+    }
+    // H1's constant features (the layer-2 bias input): X covered them
+    const uint32_t one = (uint32_t)__bfloat16_as_ushort(__float2bfloat16(1.0f));
+    *reinterpret_cast<uint4 *>(buf + act_off(t, 64, kSpH)) = make_uint4(one, 0, 0, 0);
+    *reinterpret_cast<uint4 *>(buf + act_off(t, 72, kSpH)) = make_uint4(0, 0, 0, 0);
+    handoff();
+    if (t == 0) {
+        for (int s = 0; s < (int)kK2 / 16; ++s)
+            tc::mma_bf16(d1, tc::smem_desc(tc::smem_addr(buf) + 256 * s, 128, kSpH),
+                         tc::smem_desc(tc::smem_addr(w2s) + 256 * s, 128, kSoW2), i1, s > 0);
+    }
+    sync.complete();
+    float y = b3;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        float z[32];
+        tc::tmem_ld32(tc::tmem_at(d1, 32 * warp, 32 * h), z);
+#pragma unroll
+        for (int o = 0; o < 32; ++o) y += w3[32 * h + o] * fmaxf(z[o], 0.0f);
+    }
+    return y;
+}
+
 // ---- training -------------------------------------------------------------------------------
 
 struct TrainSmem {
@@ -389,20 +433,19 @@ __device__ __forceinline__ f3 infer_input(const float4 *__restrict__ pts, const 
 // points of every ray (0 for rays with fewer than 2 SDF samples; a tile of two such rays
 // skips the MMAs).  Persistent: each CTA walks tiles of 128 points and fetches the next
 // tile's input before waiting on this tile's MMAs.
-__global__ void __launch_bounds__(128, 5) mlp_infer_kernel(const float4 *__restrict__ pts, uint32_t P,
+__global__ void __launch_bounds__(128, 6) mlp_infer_kernel(const float4 *__restrict__ pts, uint32_t P,
                                                         const qsdvr_ray_info *__restrict__ rays,
                                                         const float *__restrict__ origin,
                                                         const float *__restrict__ dir, uint32_t nrays,
                                                         float interval, const __nv_bfloat16 *__restrict__ w,
                                                         float *__restrict__ out) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t *xs = smem;
-    uint8_t *hs = xs + kBytesX;
-    uint8_t *w1s = hs + kBytesH;
+    uint8_t *xs = smem;  // X, then H1 over it (infer_tile)
+    uint8_t *w1s = xs + kBytesH;
     uint8_t *w2s = w1s + kBytesW1;
     InferSmem &S = *reinterpret_cast<InferSmem *>(w2s + kBytesW2);
     const uint32_t t = threadIdx.x, warp = t >> 5;
-    stage_weights(w, w1s, w2s, hs);
+    stage_weights(w, w1s, w2s, xs);
     if (t < 64) S.w3[t] = bf16f(w, kOffW3 + t);
     if (t == 0) tc::mbar_init(&S.mbar, 1);
     if (warp == 0) tc::tmem_alloc(&S.tmem, kInferCols);
@@ -440,11 +483,7 @@ __global__ void __launch_bounds__(128, 5) mlp_infer_kernel(const float4 *__restr
         // the next tile's input is in flight while this tile runs on the tensor cores
         if (next < tiles && gn < total) p = infer_input(pts, rays, origin, dir, interval, gn);
         live = next < tiles && gn < total && (!rays || rays[gn >> 6].sdf_count > 1);
-        float z2[kH];
-        forward_tile(xs, hs, w1s, w2s, tmem, sync, z2);
-        float y = b3;
-#pragma unroll
-        for (int o = 0; o < kH; ++o) y += S.w3[o] * fmaxf(z2[o], 0.0f);
+        const float y = infer_tile(xs, w1s, w2s, tmem, sync, S.w3, b3);
         if (valid && sync.ok) out[g] = cur_live ? softplus(y) : 0.0f;
         tile = next;
         g = gn;
@@ -626,12 +665,13 @@ __global__ void __launch_bounds__(256) proposal_draw_kernel(const qsdvr_ray_info
 }
 
 constexpr size_t train_smem() { return kBytesX + kBytesH + 2 * kBytesG + kBytesW1 + kBytesW2 + sizeof(TrainSmem); }
-constexpr size_t infer_smem() { return kBytesX + kBytesH + kBytesW1 + kBytesW2 + sizeof(InferSmem); }
+constexpr size_t infer_smem() { return kBytesH + kBytesW1 + kBytesW2 + sizeof(InferSmem); }
 // Shared memory alone keeps every resident CTA's TMEM columns free (2 training CTAs x 256
 // columns, at most 6 inference CTAs x 64), so tcgen05.alloc never has to wait in practice.
 static_assert(2 * train_smem() <= 228 * 1024 && 3 * (train_smem() + 1024) > 228 * 1024,
               "training CTAs: exactly two per SM");
 static_assert((228 * 1024 / (infer_smem() + 1024)) * kInferCols <= 512, "inference CTAs: TMEM oversubscribed");
+static_assert(6 * (infer_smem() + 1024) <= 228 * 1024, "inference CTAs: six fit per SM");
 
 // Persistent grid: resident CTAs per SM x SMs, capped at the tile count.  The occupancy API
 // answers 1 CTA per SM for kernels that use tensor memory (it cannot know how many columns a
