@@ -58,6 +58,12 @@ int qsdvr_version(void);
 /* Read (and clear when clear != 0) the device error word of the current device. */
 int qsdvr_device_error(uint32_t *word, int clear, cudaStream_t stream);
 
+/* Check of the failure path of the tensor-core kernels' bounded waits (no counterpart in the
+ * reference): one wait, limited to limit_ns (at most 2 s), on an mbarrier that no arrival
+ * completes.  It gives up, records QSDVR_DEVERR_TIMEOUT in the device error word, writes 0 to
+ * *completed (device memory) and returns; the context stays usable. */
+int qsdvr_check_bounded_wait(uint64_t limit_ns, uint32_t *completed, cudaStream_t stream);
+
 /* ---- camera (kernel/camera.cu) ----------------------------------------------------- */
 
 /* 16-byte per-ray record; include/common.h:17-23 (RayInfo), stored as int32 [N,4]. */

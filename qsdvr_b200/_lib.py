@@ -114,6 +114,10 @@ def size(name: str, *args) -> int:
     return int(getattr(lib(), name)(*args))
 
 
+# bits of the device error word (include/qsdvr_b200.h)
+QSDVR_DEVERR_INDEX, QSDVR_DEVERR_CAPACITY, QSDVR_DEVERR_RAY, QSDVR_DEVERR_TIMEOUT = 1, 2, 4, 8
+
+
 def device_error(stream=None, clear: bool = True) -> int:
     """Read (and by default clear) the device error word; synchronises the stream."""
     w = ctypes.c_uint32(0)

@@ -595,6 +595,20 @@ __global__ void __launch_bounds__(256) proposal_sample_kernel(const qsdvr_ray_in
     }
 }
 
+// ---- check of the bounded waits -------------------------------------------------------------
+// One wait, with the tensor-core kernels' own mbar_wait, on an mbarrier that no arrival ever
+// completes: it must give up after limit_ns, record QSDVR_DEVERR_TIMEOUT and return.
+__global__ void wait_check_kernel(uint64_t limit_ns, uint32_t *completed) {
+    __shared__ uint64_t mbar;
+    if (threadIdx.x == 0) tc::mbar_init(&mbar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const bool done = tc::mbar_wait(&mbar, 0, kSpins, limit_ns);
+        if (!done) flag_error(QSDVR_DEVERR_TIMEOUT);
+        *completed = done ? 1u : 0u;
+    }
+}
+
 // ---- training targets from the renderer ------------------------------------------------------
 // One warp per ray: render sample i of ray r (position midpoint(o, d, i, interval), the
 // reference's render sample) with the renderer's alpha gives the target density
@@ -795,6 +809,14 @@ extern "C" int qsdvr_proposal_sample(const qsdvr_ray_info *rays, uint32_t ray_co
                                                                                      uniform_mix, coarse_density,
                                                                                      tlist);
     return check_launch("qsdvr_proposal_sample");
+}
+
+extern "C" int qsdvr_check_bounded_wait(uint64_t limit_ns, uint32_t *completed, cudaStream_t stream) {
+    if (!completed) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_check_bounded_wait: null pointer");
+    if (limit_ns == 0 || limit_ns > 2000000000ull)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_check_bounded_wait: limit must be in (0, 2 s]");
+    wait_check_kernel<<<1, 32, 0, stream>>>(limit_ns, completed);
+    return check_launch("qsdvr_check_bounded_wait");
 }
 
 extern "C" int qsdvr_proposal_targets(const qsdvr_ray_info *rays, const float *origin, const float *dir,

@@ -79,14 +79,14 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 }
 
 // Wait for the phase with the given parity to complete; gives up after max_spins polls or
-// about two seconds, whichever comes first, and returns false (the caller records an error
-// and stops issuing work).
-__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint32_t max_spins) {
-    constexpr uint64_t kLimitNs = 2000000000ull;
+// limit_ns (about two seconds by default), whichever comes first, and returns false (the
+// caller records an error and stops issuing work).
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint32_t max_spins,
+                                          uint64_t limit_ns = 2000000000ull) {
     const uint32_t addr = smem_addr(mbar);
     const uint64_t t0 = globaltimer_ns();
     for (uint32_t i = 0; i < max_spins; ++i) {
-        if ((i & 1023u) == 1023u && globaltimer_ns() - t0 > kLimitNs) return false;
+        if ((i & 1023u) == 1023u && globaltimer_ns() - t0 > limit_ns) return false;
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

@@ -31,6 +31,7 @@ _lib.extra_signatures({
     "qsdvr_proposal_targets": [P, P, P, U32, F32, P, U64, P, P],
     "qsdvr_proposal_draw": [P, P, P, U32, F32, P, U64, U32, U32, P, P],
     "qsdvr_mlp_launch_shape": [ctypes.c_int, U32, P, P],
+    "qsdvr_check_bounded_wait": [U64, P, P],
 })
 
 INFER_MIX = 0.05  # uniform share of the fine-sample pdf when rendering

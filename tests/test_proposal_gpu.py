@@ -330,3 +330,29 @@ def test_trained_proposal_beats_same_budget_without_it(prop):
     p_prop, p_flat = _psnr(img_prop, full), _psnr(img_flat, full)
     print(f"PSNR vs 512-sample march: proposal {p_prop:.2f} dB, uniform-32 {p_flat:.2f} dB")
     assert p_prop > p_flat + 3.0
+
+
+def test_bounded_wait_gives_up_and_reports(prop):
+    """The tensor-core kernels' mbarrier waits are bounded: a wait that nothing completes gives
+    up after its limit (10 ms here), sets QSDVR_DEVERR_TIMEOUT and returns, and the context
+    stays usable (an MLP launch right after still matches the oracle)."""
+    import ctypes
+    import time
+
+    from qsdvr_b200 import _lib
+    from qsdvr_b200._lib import QSDVR_DEVERR_TIMEOUT, call
+
+    assert _lib.device_error() == 0
+    done = torch.full((1,), 7, dtype=torch.int32, device=DEV)
+    stream = torch.cuda.current_stream()
+    t0 = time.perf_counter()
+    call("qsdvr_check_bounded_wait", 10_000_000, done.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
+    torch.cuda.synchronize()
+    elapsed = time.perf_counter() - t0
+    assert int(done.item()) == 0
+    assert 0.005 < elapsed < 1.0
+    assert _lib.device_error() & QSDVR_DEVERR_TIMEOUT
+    assert _lib.device_error() == 0  # read and cleared
+    w, pts = _params(), _points(300)
+    got = _net(prop, w).density(torch.from_numpy(pts).to(DEV)).cpu().numpy()
+    assert _close(got, OP.density(w.numpy(), pts), 1e-3, 1e-3) <= 1.0
