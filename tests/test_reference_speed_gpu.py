@@ -6,9 +6,11 @@ lists that its dataset precomputes per batch (datasets/utils.py:17-33): SampleSD
 SampleNormal, GridInterpolation, Shader and RayAggregate forward, then their backward ops,
 each Function's backward allocating zeroed dense gradient grids (models/render.py:28-33,
 136-146, 160-169).  Timed here: exactly that chain (forward + MSE gradient + backward, with
-the dense zero-fills), against zero-fill + one fused train launch.  Both see identical rays,
-grids and targets; the reference's colours and gradients are also checked against ours so
-the two timed computations are the same work.  Prints one JSON line."""
+the dense zero-fills), against zero-fill + one fused train launch, and against the same op
+chain run through this library's drop-in ``qsdvr`` module (same function names and
+arguments, this library's per-op kernels).  All three see identical rays, grids and
+targets; the reference's colours and gradients are checked against both of ours so the timed
+computations are the same work.  Prints one JSON line."""
 import json
 
 import pytest
@@ -85,14 +87,19 @@ def test_fused_train_faster_than_reference_chain():
 
     ref_ms = _time(lambda: reference_render(ref, grid7, data, inp, R, k, target))
     our_ms = _time(ours)
+    dropin_ms = _time(lambda: reference_render(qsdvr, grid7, data, inp, R, k, target))
+    img2, g72, gd2 = reference_render(qsdvr, grid7, data, inp, R, k, target)
     img, g7, gd = reference_render(ref, grid7, data, inp, R, k, target)
     ours()
     col = fused.render_forward(r, o, d, grid8, data, R, interval, k)
     torch.cuda.synchronize()
     assert (col - img).abs().max().item() < 1e-5
     assert rel_err(sg[:, :7].cpu(), g7.cpu()) < 1e-4 and rel_err(dg.cpu(), gd.cpu()) < 1e-4
+    assert (img2 - img).abs().max().item() < 1e-5
+    assert rel_err(g72.cpu(), g7.cpu()) < 1e-4 and rel_err(gd2.cpu(), gd.cpu()) < 1e-4
     print(json.dumps({"workload": "R=256 fp32 compat, 65536 rays from 800^2 views, 256 samples/ray",
                       "render_samples": M, "reference_cuda_ms": round(ref_ms, 3), "fused_ms": round(our_ms, 3),
                       "reference_rays_per_s": round(n_rays / ref_ms * 1e3), "fused_rays_per_s":
-                      round(n_rays / our_ms * 1e3), "speedup": round(ref_ms / our_ms, 2)}))
+                      round(n_rays / our_ms * 1e3), "speedup": round(ref_ms / our_ms, 2),
+                      "dropin_op_chain_ms": round(dropin_ms, 3), "dropin_speedup": round(ref_ms / dropin_ms, 2)}))
     assert our_ms < ref_ms
