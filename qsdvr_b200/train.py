@@ -15,6 +15,11 @@ with it).  The network is trained online every step on the per-sample alphas of 
 uniform-march forward over part of the batch.
 Held-out PSNR is always measured with the uniform march.
 
+``--model separable`` trains the reference's own parametrisation instead of a dense quadric
+grid: the three per-axis layers and the offset of models/render.py:172-207 (Adam, as
+test.py:20) with the appearance grid (fused Adam), through the fused kernels that assemble
+cells from the layers' tables.
+
 ``--save PATH`` writes a checkpoint (checkpoint.py) at the end and every ``--save-every``
 steps; ``--resume PATH`` continues a run from one, with the same ray batches as the run that
 was not interrupted.
@@ -81,6 +86,8 @@ def parser():
     ap.add_argument("--save", default=None, help="checkpoint path written at the end (and every --save-every)")
     ap.add_argument("--save-every", type=int, default=0)
     ap.add_argument("--resume", default=None, help="checkpoint to continue from (steps counts the total)")
+    ap.add_argument("--model", default="dense", choices=["dense", "separable"],
+                    help="dense quadric grid, or the reference's separable layers (RenderGrid)")
     ap.add_argument("--seed", type=int, default=0)
     return ap
 
@@ -97,6 +104,8 @@ def run(a, data=None, quiet=False, return_state=False):
     R = a.reso
     if data is None:
         data = build(R, a.views, a.size, 1111.1 * a.size / 800, 4.03, a.interval, a.k, a.seed, dev, a.sh)
+    if getattr(a, "model", "dense") == "separable":
+        return run_separable(a, data, quiet, return_state)
     rays, origin, direction, target = data
     total = rays.shape[0]
     gen = torch.Generator(device=dev).manual_seed(a.seed + 1)
@@ -185,6 +194,70 @@ def run(a, data=None, quiet=False, return_state=False):
     if not quiet:
         print(json.dumps(out), flush=True)
     return (out, model, net) if return_state else out
+
+
+def run_separable(a, data, quiet=False, return_state=False):
+    """The training loop of ``run`` for the reference's separable model (SeparableRenderGrid):
+    one fused forward + MSE + backward launch per step, then Adam on the layers and the
+    offset and the fused Adam on the appearance grid."""
+    if a.proposal or a.online_proposal or a.sh != 2 or a.storage != "f32" or a.save or a.resume:
+        raise ValueError("--model separable trains the reference's fp32 SH-2 model with the uniform march only")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    R = a.reso
+    rays, origin, direction, target = data
+    total = rays.shape[0]
+    gen = torch.Generator(device=dev).manual_seed(a.seed + 1)
+    held = torch.randint(0, total, (a.rays,), generator=gen, device=dev)
+    torch.cuda.reset_peak_memory_stats(dev)
+    base_mem = torch.cuda.memory_allocated(dev)
+    model = fused.SeparableRenderGrid(R, a.k, a.interval, mode=a.mode, device=dev)
+    layers = [model.xLayer, model.yLayer, model.zLayer, model.offset]
+    opt_layers = torch.optim.Adam(layers, lr=a.lr)
+    opt_grid = FusedGridAdam([model.renderData], lr=a.lr)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+
+    def evaluate():
+        with torch.no_grad():
+            col = model(rays[held], origin[held], direction[held])
+        return float(((col - target[held]) ** 2).mean())
+
+    start = evaluate()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    log = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for step in range(1, a.steps + 1):
+        idx = torch.randint(0, total, (a.rays,), generator=gen, device=dev)
+        e0, e1, e2 = ev[step - 1]
+        e0.record()
+        loss.zero_()
+        model.train_step(target[idx], rays[idx], origin[idx], direction[idx], loss=loss)
+        e1.record()
+        opt_grid.step()  # fused Adam on the appearance grid; zeroes its gradient
+        opt_layers.step()
+        opt_layers.zero_grad(set_to_none=True)
+        e2.record()
+        if not quiet and (step % a.log_every == 0 or step == a.steps):
+            torch.cuda.synchronize()
+            log.append({"step": step, "train_mse": float(loss) / (3 * a.rays),
+                        "elapsed_s": round(time.perf_counter() - t0, 3)})
+            print(json.dumps(log[-1]), flush=True)
+    torch.cuda.synchronize()
+    elapsed = time.perf_counter() - t0
+    render_ms = sum(x.elapsed_time(y) for x, y, _ in ev)
+    opt_ms = sum(y.elapsed_time(z) for _, y, z in ev)
+    end = evaluate()
+    out = {"model": "separable (reference RenderGrid layers)", "reso": R, "steps": a.steps, "rays_per_step": a.rays,
+           "lr": a.lr, "mode": a.mode, "k": a.k, "ms_per_step": round(1e3 * elapsed / a.steps, 3),
+           "train_rays_per_s": round(a.steps * a.rays / elapsed), "render_ms": round(render_ms, 3),
+           "optimizer_ms": round(opt_ms, 3), "render_rays_per_s": round(a.steps * a.rays / (render_ms / 1e3)),
+           "heldout_psnr_start": round(psnr(start), 3), "heldout_psnr_end": round(psnr(end), 3),
+           "peak_memory_gb": round(torch.cuda.max_memory_allocated(dev) / 1e9, 3),
+           "model_and_state_gb": round((torch.cuda.max_memory_allocated(dev) - base_mem) / 1e9, 3)}
+    if not quiet:
+        print(json.dumps(out), flush=True)
+    return (out, model, None) if return_state else out
 
 
 def main(argv=None):

@@ -148,3 +148,20 @@ def test_separable_autograd_matches_train_step(qs):
     assert (col - img.detach()).abs().max().item() < 1e-6
     for p, q in zip(a.parameters(), b.parameters()):
         assert rel_err(p.grad.cpu(), q.grad.cpu()) < 1e-5
+
+
+def test_separable_training_driver_improves_heldout_psnr():
+    """train.py --model separable: the reference's own parametrisation (layers + offset +
+    appearance grid) trained through the fused kernels improves the held-out PSNR."""
+    from qsdvr_b200 import train
+
+    a = train.parser().parse_args([])
+    a.model, a.reso, a.views, a.size, a.rays, a.steps = "separable", 32, 3, 48, 2048, 40
+    a.interval, a.log_every = 4.0 / 96, 10 ** 9
+    out = train.run(a, quiet=True)
+    # measured +0.8 dB at these settings: the separable SDF (a sum of three 1-D piecewise
+    # quadratics) fits the procedural scene far less than a dense grid does
+    assert out["heldout_psnr_end"] > out["heldout_psnr_start"] + 0.3, out
+    from qsdvr_b200 import _lib
+
+    assert _lib.device_error() == 0
