@@ -290,13 +290,16 @@ def run_ours(args, cfg, device, ws, rank):
     # gradients accumulate over the steps into buffers zeroed once before timing (the
     # scatter's work does not depend on what the buffers hold); zeroing and the optimizer
     # step are timed separately below, and a full training step beside them
+    # each step takes its rays in the Morton order of their midpoints (keys + sort inside the
+    # timed step; the kernel events bracket the train launch alone)
     def step(i, ev):
         b = batches[i % len(batches)]
         loss.zero_()
+        order = fused.ray_order(b["rays"], b["origin"], b["dir"], cfg["interval"])
         if ev is not None:
             ev[0].record(stream)
         fused.render_train(b["target"], b["rays"], b["origin"], b["dir"], sdf_k, data_k, R, cfg["interval"],
-                           K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color)
+                           K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color, order=order)
         if ev is not None:
             ev[1].record(stream)
 
@@ -333,8 +336,10 @@ def run_ours(args, cfg, device, ws, rank):
         stream.wait_event(copied[i % 2])
         if ev is not None:
             ev[0].record(stream)
+        order = fused.ray_order(buf["rays"], buf["origin"], buf["dir"], cfg["interval"])
         fused.render_train(buf["target"], buf["rays"], buf["origin"], buf["dir"], sdf_k, data_k, R,
-                           cfg["interval"], K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color)
+                           cfg["interval"], K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color,
+                           order=order)
         if ev is not None:
             ev[1].record(stream)
         released[i % 2].record(stream)
@@ -371,12 +376,13 @@ def run_ours(args, cfg, device, ws, rank):
                                f"interval {cfg['interval']:.6g} (256 samples/ray), SH degree {cfg.get('sh', 2)}, "
                                f"{mode} mode, k={K_LOGISTIC}",
                    "global_batch": cfg["rays"] * ws, "samples_per_step": round(mean_samples),
-                   "step": "one fused forward/MSE/backward launch, gradients accumulated into buffers zeroed "
+                   "step": "ray-order keys + sort (rays taken in Morton order of their midpoints), then one "
+                           "fused forward/MSE/backward launch; gradients accumulated into buffers zeroed "
                            "before the timed region (zeroing, optimizer and full step in step_parts)",
                    "l2": "inputs larger than L2 (grids 2.7 GB), no flush", "parallelism": f"replicas x{ws}"},
         "e2e": {"value": round(e2e_value, 1), "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4,
                 "wall_s": round(wall_e2e, 3)},
-        "gpu_launches": args.steps,
+        "gpu_launches": 2 * args.steps,  # qsdvr_ray_order_keys + the train kernel per step
         "step_parts": step_parts,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None if traffic is None else round(traffic),
@@ -430,8 +436,9 @@ def full_step_parts(args, cfg, batches, sdf, data, sdf_k, data_k, sg, dg, mode, 
     def full():
         b = batches[count[0] % len(batches)]
         loss.zero_()
+        order = fused.ray_order(b["rays"], b["origin"], b["dir"], cfg["interval"])
         fused.render_train(b["target"], b["rays"], b["origin"], b["dir"], sdf_k, data_k, cfg["R"], cfg["interval"],
-                           K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color)
+                           K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color, order=order)
         adam()
 
     full_ms = timed(full, max(3, args.steps // 2))

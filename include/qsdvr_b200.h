@@ -244,7 +244,18 @@ typedef struct qsdvr_render_args {
     float *sample_alpha;      /* optional: alpha of render sample i of ray r written at
                                  rays[r].render_offset + i (forward and train)                   */
     uint64_t sample_capacity; /* length of sample_alpha */
+    const uint32_t *order;    /* optional [ray_count]: the order in which the persistent kernel
+                                 takes the rays (a permutation of 0..ray_count-1, e.g. rays sorted
+                                 by qsdvr_ray_order_keys); outputs stay indexed by ray          */
 } qsdvr_render_args;
+
+/* Sort keys that make neighbouring rays in a batch cross neighbouring cells (no counterpart
+ * in the reference): the 30-bit Morton code of each ray's in-box midpoint on a 1024^3 lattice
+ * of the volume, 0x7fffffff for rays with fewer than 2 SDF samples (keys sort the same signed
+ * or unsigned).  Rays taken in key order
+ * by qsdvr_render_* (args.order) share more gathered rows and gradient lines in L2. */
+int qsdvr_ray_order_keys(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
+                         float interval, uint32_t *keys, cudaStream_t stream);
 
 /* Separable SDF for the fused renderer (the RenderGrid model's parametrisation,
  * models/render.py:172-207, without materialising [R^3][7]; LayerToGridForward,

@@ -111,6 +111,7 @@ struct Params {
     const float *tlist;     // list sampling: per ray kListT SDF positions (t from origin), or null
     float *sample_alpha;    // optional per-render-sample alpha output (forward, train)
     uint64_t sample_capacity;
+    const uint32_t *order;  // optional: the i-th ray taken is order[i]
 };
 
 constexpr uint32_t kListT = 33;  // list sampling: 33 SDF positions, 32 render samples per ray
@@ -669,6 +670,15 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
         r = __shfl_sync(kFull, t, 0);
     }
     if (r >= p.n) break;
+    const uint32_t taken = r;  // the ray counter's index; the ray itself may come from an order
+    if (p.order) {
+        r = p.order[taken];
+        if (r >= p.n) {  // not a permutation of the batch: skip the entry
+            if (lane == 0) flag_error(QSDVR_DEVERR_RAY);
+            if (!persistent) break;
+            continue;
+        }
+    }
     {
         const qsdvr_ray_info info = p.rays[r];
         const uint32_t ns = info.sdf_count;
@@ -958,6 +968,7 @@ int launch(const qsdvr_render_args *a, cudaStream_t stream) {
     p.tlist = a->tlist;
     p.sample_alpha = a->sample_alpha;
     p.sample_capacity = a->sample_capacity;
+    p.order = a->order;
     unsigned blocks = grid_for(a->ray_count, kWarpsPerBlock);
     if (a->workspace) {
         const Layout L = layout_for(a, kPass);
@@ -1015,7 +1026,53 @@ int validate(const qsdvr_render_args *a, int pass) {
 }  // namespace
 }  // namespace qsdvr
 
+namespace qsdvr {
+namespace {
+
+// 10 bits of v spread to every third bit.
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__global__ void __launch_bounds__(256) ray_order_keys_kernel(const qsdvr_ray_info *__restrict__ rays,
+                                                             const float *__restrict__ origin,
+                                                             const float *__restrict__ dir, uint32_t n,
+                                                             float interval, uint32_t *__restrict__ keys) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint32_t ns = rays[r].sdf_count;
+    if (ns < 2) {
+        keys[r] = 0x7fffffffu;  // after every ray with samples, also as a signed key
+        return;
+    }
+    const float t = 0.5f * (float)(ns - 1) * interval;  // the in-box segment's midpoint
+    const f3 o = load3(origin + 3ull * r), d = load3(dir + 3ull * r);
+    const float c[3] = {fmaf(d.x, t, o.x), fmaf(d.y, t, o.y), fmaf(d.z, t, o.z)};
+    uint32_t q[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) q[a] = (uint32_t)fminf(fmaxf((c[a] + 1.0f) * 512.0f, 0.0f), 1023.0f);
+    keys[r] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+}
+
+}  // namespace
+}  // namespace qsdvr
+
 using namespace qsdvr;
+
+extern "C" int qsdvr_ray_order_keys(const qsdvr_ray_info *rays, const float *origin, const float *dir,
+                                    uint32_t ray_count, float interval, uint32_t *keys, cudaStream_t stream) {
+    if (ray_count == 0) return QSDVR_OK;
+    if (!rays || !origin || !dir || !keys)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_order_keys: null pointer");
+    if (!(interval > 0.0f)) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_order_keys: interval must be > 0");
+    ray_order_keys_kernel<<<grid_for(ray_count, 256), 256, 0, stream>>>(rays, origin, dir, ray_count, interval, keys);
+    return check_launch("qsdvr_ray_order_keys");
+}
 
 extern "C" size_t qsdvr_render_workspace_size(const qsdvr_render_args *args) {
     if (!args) return 0;

@@ -33,7 +33,7 @@ class RenderArgs(ctypes.Structure):
                 ("sdf_grid", P), ("data", P), ("color", P), ("target", P), ("grad_color", P), ("sdf_grad", P),
                 ("data_grad", P), ("loss", P), ("grad_scale", F32), ("workspace", P), ("workspace_bytes", ctypes.c_uint64),
                 ("sdf_layers", P), ("sdf_layers_grad", P), ("tlist", P), ("sample_alpha", P),
-                ("sample_capacity", ctypes.c_uint64)]
+                ("sample_capacity", ctypes.c_uint64), ("order", P)]
 
 
 _lib.extra_signatures({
@@ -42,6 +42,7 @@ _lib.extra_signatures({
     "qsdvr_render_train": [ctypes.POINTER(RenderArgs), P],
     "qsdvr_separable_sdf_tables": [P, P, P, P, U32, P, P],
     "qsdvr_separable_sdf_grad": [P, U32, P, P, P, P, P],
+    "qsdvr_ray_order_keys": [P, P, P, U32, F32, P, P],
 }, {"qsdvr_render_workspace_size": [ctypes.POINTER(RenderArgs)]})
 
 _workspaces: dict = {}
@@ -99,7 +100,7 @@ def _grid_storage(sdf_grid, data, R):
 def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat", transmittance="product",
               color=None, target=None, grad_color=None, sdf_grad=None, data_grad=None, loss=None,
               grad_scale=0.0, persistent=True, tlist=None, sample_alpha=None, sdf_layers=None,
-              sdf_layers_grad=None) -> RenderArgs:
+              sdf_layers_grad=None, order=None) -> RenderArgs:
     dev, n = _check_batch(rays, origin, direction)
     a = RenderArgs()
     a.rays, a.origin, a.dir = _ptr(rays), _ptr(origin), _ptr(direction)
@@ -134,6 +135,10 @@ def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="
         if sample_alpha.device != dev or sample_alpha.dtype != torch.float32 or not sample_alpha.is_contiguous():
             raise ValueError(f"sample_alpha must be a contiguous float32 tensor on {dev}")
         a.sample_alpha, a.sample_capacity = _ptr(sample_alpha), sample_alpha.numel()
+    if order is not None:
+        if order.device != dev or order.dtype != torch.int32 or order.shape != (n,) or not order.is_contiguous():
+            raise ValueError(f"order must be a contiguous int32 [N] permutation on {dev}")
+        a.order = order.data_ptr()
     if persistent and n:
         with torch.cuda.device(dev):
             ws = workspace(dev, a)
@@ -145,25 +150,40 @@ def _stream(dev):
     return ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
 
 
+def ray_order(rays, origin, direction, interval) -> torch.Tensor:
+    """A permutation (int32 [N]) that lists the rays by the Morton code of their in-box
+    midpoint (qsdvr_ray_order_keys), rays without samples last.  Passed as ``order`` to the
+    render calls, neighbouring rays in the kernel's schedule cross neighbouring cells, so more
+    of the gathered rows and gradient lines are found in L2."""
+    dev, n = _check_batch(rays, origin, direction)
+    keys = torch.empty(n, dtype=torch.int32, device=dev)
+    with torch.cuda.device(dev):
+        call("qsdvr_ray_order_keys", _ptr(rays), _ptr(origin), _ptr(direction), n, float(interval), _ptr(keys),
+             _stream(dev))
+    return torch.argsort(keys).to(torch.int32)
+
+
 def render_forward(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat",
                    transmittance="product", color=None, persistent=True, tlist=None, sample_alpha=None,
-                   sdf_layers=None):
+                   sdf_layers=None, order=None):
     """Colour of every ray [N,3].  ``tlist`` [N,33]: render at those SDF positions (32 render
     samples per ray at their midpoints) instead of the uniform march; ``sample_alpha``: also
     write every render sample's alpha at the ray's render offset; ``sdf_layers`` (with
-    ``sdf_grid`` None): the separable SDF tables of ``separable_tables``."""
+    ``sdf_grid`` None): the separable SDF tables of ``separable_tables``; ``order``: the
+    order in which the kernel takes the rays (``ray_order``)."""
     dev, n = _check_batch(rays, origin, direction)
     if color is None:
         color = torch.empty((n, 3), dtype=torch.float32, device=dev)
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color,
-                  persistent=persistent, tlist=tlist, sample_alpha=sample_alpha, sdf_layers=sdf_layers)
+                  persistent=persistent, tlist=tlist, sample_alpha=sample_alpha, sdf_layers=sdf_layers, order=order)
     with torch.cuda.device(dev):
         call("qsdvr_render_forward", ctypes.byref(a), _stream(dev))
     return color
 
 
 def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
-                    mode="compat", transmittance="product", persistent=True, tlist=None, sdf_layers=None):
+                    mode="compat", transmittance="product", persistent=True, tlist=None, sdf_layers=None,
+                    order=None):
     """Accumulate dL/d(sdf_grid) and dL/d(data) (fp32) for a given dL/dcolor.  With
     ``sdf_layers``, ``sdf_grad`` is the tables' gradient ([3R+1,4], see ``separable_grad``)."""
     dev, n = _check_batch(rays, origin, direction)
@@ -175,14 +195,14 @@ def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, i
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, grad_color=g,
                   sdf_grad=None if sdf_layers is not None else sdf_grad, data_grad=data_grad,
                   persistent=persistent, tlist=tlist, sdf_layers=sdf_layers,
-                  sdf_layers_grad=sdf_grad if sdf_layers is not None else None)
+                  sdf_layers_grad=sdf_grad if sdf_layers is not None else None, order=order)
     with torch.cuda.device(dev):
         call("qsdvr_render_backward", ctypes.byref(a), _stream(dev))
 
 
 def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
                  mode="compat", transmittance="product", loss=None, color=None, persistent=True, tlist=None,
-                 sample_alpha=None, sdf_layers=None):
+                 sample_alpha=None, sdf_layers=None, order=None):
     """Forward + MSE (mean over N x 3) + backward in one launch.  Returns (color, loss_sum)
     where loss_sum accumulates sum |color - target|^2 (divide by 3N for the mean).  With
     ``sdf_layers``, ``sdf_grad`` is the tables' gradient ([3R+1,4])."""
@@ -195,7 +215,8 @@ def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, color=color,
                   target=target.contiguous(), sdf_grad=None if sep else sdf_grad, data_grad=data_grad, loss=loss,
                   grad_scale=2.0 / (3.0 * max(n, 1)), persistent=persistent, tlist=tlist,
-                  sample_alpha=sample_alpha, sdf_layers=sdf_layers, sdf_layers_grad=sdf_grad if sep else None)
+                  sample_alpha=sample_alpha, sdf_layers=sdf_layers, sdf_layers_grad=sdf_grad if sep else None,
+                  order=order)
     with torch.cuda.device(dev):
         call("qsdvr_render_train", ctypes.byref(a), _stream(dev))
     return color, loss

@@ -86,6 +86,8 @@ def parser():
     ap.add_argument("--save", default=None, help="checkpoint path written at the end (and every --save-every)")
     ap.add_argument("--save-every", type=int, default=0)
     ap.add_argument("--resume", default=None, help="checkpoint to continue from (steps counts the total)")
+    ap.add_argument("--no-ray-order", dest="ray_order", action="store_false",
+                    help="take each batch's rays in batch order instead of the Morton order of their midpoints")
     ap.add_argument("--model", default="dense", choices=["dense", "separable"],
                     help="dense quadric grid, or the reference's separable layers (RenderGrid)")
     ap.add_argument("--seed", type=int, default=0)
@@ -156,8 +158,9 @@ def run(a, data=None, quiet=False, return_state=False):
                             points=a.proposal_points)
             if a.proposal and step > a.proposal_warmup:
                 tlist = net.sample(r, o, d, a.interval, a.proposal_mix)
+        order = fused.ray_order(r, o, d, a.interval) if a.ray_order else None
         fused.render_train(tg, r, o, d, sg, dg, R, a.interval, a.k, model.sdfGrid.grad, model.renderData.grad,
-                           a.mode, model.transmittance, loss=loss, tlist=tlist)
+                           a.mode, model.transmittance, loss=loss, tlist=tlist, order=order)
         e1.record()
         opt.step()  # Adam on the fp32 masters; zeroes the gradients, refreshes bf16 copies
         e2.record()

@@ -245,3 +245,51 @@ def test_fused_sh_degree3_vs_oracle(fz, storage):
     assert rel_err(sg[:, :7].cpu(), wg) < GRAD_TOL
     assert rel_err(dg.cpu(), wd) < GRAD_TOL
     assert float(dg[:, 53:].abs().max()) == 0.0  # unused channels get no gradient
+
+
+def test_ray_order_gives_same_results(fz):
+    """Rays taken in Morton order of their midpoints (qsdvr_ray_order_keys + args.order) give
+    the same colours, loss and gradients as the batch order; the keys are the 30-bit Morton
+    codes of the midpoints (rays without samples last); an order entry outside the batch is
+    skipped and flagged, not read."""
+    import numpy as np
+
+    from qsdvr_b200 import _lib, scenes
+
+    R, k, interval = 32, 8.0, 4.0 / 96
+    cam = camera_batch((1.9, -3.1, 1.4), 56, 75.0, interval, R)
+    grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.55, 0.01, seed=11).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=11).to(DEV)
+    n = cam.rayList.shape[0]
+    target = torch.rand((n, 3), generator=torch.Generator().manual_seed(12)).to(DEV)
+    args = (cam.rayList, cam.originList, cam.dirList)
+    order = fz.ray_order(*args, interval)
+    assert torch.equal(order.sort().values.cpu(), torch.arange(n, dtype=torch.int32))
+    # keys: Morton code of the in-box midpoint on a 1024^3 lattice
+    r, o, d = (t.cpu().numpy() for t in args)
+    ns = r[:, 0].astype(np.int64)
+    t = 0.5 * (ns - 1).astype(np.float32) * np.float32(interval)
+    mid = o + d * t[:, None]
+    q = np.clip(np.floor((mid + 1.0) * 512.0), 0, 1023).astype(np.int64)
+    key = np.zeros(n, np.int64)
+    for b in range(10):
+        for a in range(3):
+            key |= ((q[:, a] >> b) & 1) << (3 * b + a)
+    key[ns < 2] = 0x7FFFFFFF
+    got = order.cpu().numpy()
+    ks = key[got]
+    assert np.all(np.diff(ks) >= 0) or np.mean(np.diff(ks) >= 0) > 0.999  # float rounding at lattice edges
+    out = []
+    for o_ in (None, order):
+        sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+        col, loss = fz.render_train(target, *args, grid8, data, R, interval, k, sg, dg, mode="fixed", order=o_)
+        out.append((col, loss, sg, dg))
+    (c0, l0, s0, d0), (c1, l1, s1, d1) = out
+    assert (c0 - c1).abs().max().item() < 1e-6
+    assert abs(l0.item() - l1.item()) <= n * 2.0 ** -24 * max(1.0, l0.item())
+    assert rel_err(s1.cpu(), s0.cpu()) < 1e-5 and rel_err(d1.cpu(), d0.cpu()) < 1e-5
+    assert _lib.device_error() == 0
+    bad = order.clone()
+    bad[0] = n + 5
+    fz.render_forward(*args, grid8, data, R, interval, k, "fixed", order=bad)
+    assert _lib.device_error() & _lib.QSDVR_DEVERR_RAY
