@@ -41,6 +41,9 @@ WORKLOADS = {
                      storage="f32"),
     "bf16_256": dict(R=256, rays=65536, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
                      storage="bf16"),
+    # the precision form with the appearance gradient accumulated in bf16 (SDF gradient fp32)
+    "bf16g_256": dict(R=256, rays=65536, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
+                      storage="bf16", grad="bf16"),
     "plain128": dict(R=128, rays=8192, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
                      storage="f32"),
     # SH degree 3 (64-channel rows, fixed mode): the configs' appearance model
@@ -66,12 +69,14 @@ WORKLOADS = {
 PROPOSAL_STEPS = 300  # training steps per method in the default line's proposal comparison
 
 
-def bytes_per_sample(storage: str, sh: int) -> int:
+def bytes_per_sample(storage: str, sh: int, grad: str = "f32") -> int:
     """Algorithmic bytes per render sample (3-pass model): forward gather 8 C b, backward
-    re-gather 8 C b, gradient scatter 8 C 4, quadric cells 192 (C channels, b storage bytes)."""
+    re-gather 8 C b, gradient scatter 8 C g, quadric cells 192 (C channels, b storage bytes,
+    g gradient bytes)."""
     c = 32 if sh == 2 else 64
     b = 4 if storage == "f32" else 2
-    return 8 * c * b * 2 + 8 * c * 4 + 192
+    g = 4 if grad == "f32" else 2
+    return 8 * c * b * 2 + 8 * c * g + 192
 BYTES_PER_RAY = 64  # origin + dir in, target in, colour out, RayInfo
 K_LOGISTIC = 5.0
 METRIC = "train rays/s fwd+bwd @256^3 grid (256 samples/ray, 65536-ray batches)"
@@ -282,7 +287,8 @@ def run_ours(args, cfg, device, ws, rank):
     else:
         sdf_k, data_k = sdf, data
     sg = torch.zeros(sdf.shape, dtype=torch.float32, device=device)
-    dg = torch.zeros(data.shape, dtype=torch.float32, device=device)
+    grad_dtype = torch.bfloat16 if cfg.get("grad", "f32") == "bf16" else torch.float32
+    dg = torch.zeros(data.shape, dtype=grad_dtype, device=device)
     loss = torch.zeros(1, dtype=torch.float32, device=device)
     color = torch.empty((cfg["rays"], 3), dtype=torch.float32, device=device)
     stream = torch.cuda.current_stream(device)
@@ -359,16 +365,19 @@ def run_ours(args, cfg, device, ws, rank):
     # ---- roofline of the train kernel
     samples = [samples_of(b) for b in batches]
     mean_samples = sum(samples) / len(samples)
-    bps = bytes_per_sample(storage, cfg.get("sh", 2))
+    bps = bytes_per_sample(storage, cfg.get("sh", 2), cfg.get("grad", "f32"))
     alg_bytes = mean_samples * bps + cfg["rays"] * BYTES_PER_RAY
     achieved = alg_bytes / (kern_avg / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    tps = profiled_traffic_per_sample(storage + ("_sh3" if cfg.get("sh", 2) == 3 else ""))
+    tps = profiled_traffic_per_sample(storage + ("_sh3" if cfg.get("sh", 2) == 3 else "")
+                                      + ("_grad_bf16" if cfg.get("grad", "f32") == "bf16" else ""))
     traffic = None if tps is None else tps * mean_samples
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "rays/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if storage == "f32" else "bf16 storage, f32 math",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if storage == "f32" else ("bf16 storage, f32 math" + (", bf16 appearance gradient"
+                                                                          if cfg.get("grad") == "bf16" else "")),
         "data": "synthetic (seeded procedural scene, random-init sphere model)",
         "config": {"workload": f"{args.workload}: R={R}^3 quadric + ({R + 1})^3x{32 if cfg.get('sh', 2) == 2 else 64} "
                                f"appearance grid, {storage}, "

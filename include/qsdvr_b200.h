@@ -247,6 +247,10 @@ typedef struct qsdvr_render_args {
     const uint32_t *order;    /* optional [ray_count]: the order in which the persistent kernel
                                  takes the rays (a permutation of 0..ray_count-1, e.g. rays sorted
                                  by qsdvr_ray_order_keys); outputs stay indexed by ray          */
+    int32_t data_grad_storage; /* QSDVR_STORAGE_F32 (default) or QSDVR_STORAGE_BF16: data_grad
+                                  accumulated as bf16 (each contribution and each sum rounded to
+                                  8 significant bits, half the gradient traffic); no reference
+                                  counterpart.  The SDF gradient stays fp32.                     */
 } qsdvr_render_args;
 
 /* Sort keys that make neighbouring rays in a batch cross neighbouring cells (no counterpart
@@ -290,7 +294,8 @@ int qsdvr_render_train(const qsdvr_render_args *args, cudaStream_t stream);
 
 enum {
     QSDVR_ADAM_ZERO_GRAD = 1,      /* write zeros over the gradient after using it           */
-    QSDVR_ADAM_SKIP_ZERO_GRAD = 2  /* leave elements whose gradient is exactly 0 untouched    */
+    QSDVR_ADAM_SKIP_ZERO_GRAD = 2, /* leave elements whose gradient is exactly 0 untouched    */
+    QSDVR_ADAM_GRAD_BF16 = 4       /* grad points to bf16 values (render data_grad_storage)  */
 };
 
 /* One Adam step over `count` fp32 elements.  The default (flags without SKIP_ZERO_GRAD)
@@ -299,7 +304,7 @@ enum {
  * storage copy the fused render kernels read). */
 typedef struct qsdvr_adam_args {
     float *param;
-    float *grad;
+    float *grad;        /* fp32, or bf16 with QSDVR_ADAM_GRAD_BF16 */
     float *exp_avg;
     float *exp_avg_sq;
     void *param_bf16;   /* optional [count] bf16 */

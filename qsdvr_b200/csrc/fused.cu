@@ -112,6 +112,7 @@ struct Params {
     float *sample_alpha;    // optional per-render-sample alpha output (forward, train)
     uint64_t sample_capacity;
     const uint32_t *order;  // optional: the i-th ray taken is order[i]
+    bool grad_bf16;         // data_grad holds bf16 values
 };
 
 constexpr uint32_t kListT = 33;  // list sampling: 33 SDF positions, 32 render samples per ray
@@ -126,6 +127,10 @@ __device__ __forceinline__ f3 at_t(f3 o, f3 d, float t) {
 
 __device__ __forceinline__ float bf_lo(uint32_t v) { return __uint_as_float(v << 16); }
 __device__ __forceinline__ float bf_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
 
 template <typename S>
 struct Store;
@@ -614,8 +619,15 @@ struct Transmittance {
     }
 };
 
+// 4 channels of the bf16 data gradient: one 8-byte vector RED (bf16x2 pairs, noftz).
+__device__ __forceinline__ void red4_bf16(__nv_bfloat16 *p, float4 v) {
+    const uint32_t lo = pack_bf16x2(v.x, v.y), hi = pack_bf16x2(v.z, v.w);
+    asm volatile("red.global.add.noftz.v2.bf16x2 [%0], {%1, %2};" ::"l"(p), "r"(lo), "r"(hi) : "memory");
+}
+
 // Scatter the data-gradient tile (rows of 32 channels per lane's sample) through the
-// trilinear weights: 8 lanes per sample, one 16-byte RED per lane and corner.
+// trilinear weights: 8 lanes per sample, one 16-byte RED (8 bytes for a bf16 gradient) per
+// lane and corner.
 template <int kDeg>
 __device__ __forceinline__ void scatter_tile(const Params &p, const float *tile, const Sample &s, int lane) {
     using RW = Rows<kDeg>;
@@ -635,15 +647,20 @@ __device__ __forceinline__ void scatter_tile(const Params &p, const float *tile,
         const float dx = 1 - px, dy = 1 - py;
         const float4 a0 = scale4(g, 1 - pz), a1 = scale4(g, pz);
         const float4 a00 = scale4(a0, dy), a01 = scale4(a0, py), a10 = scale4(a1, dy), a11 = scale4(a1, py);
-        float *b = p.data_grad + (uint64_t)kC * vb + 4 * q;
-        red4(b, scale4(a00, dx));
-        red4(b + kC, scale4(a00, px));
-        red4(b + (uint64_t)kC * sy, scale4(a01, dx));
-        red4(b + (uint64_t)kC * sy + kC, scale4(a01, px));
-        red4(b + (uint64_t)kC * sz, scale4(a10, dx));
-        red4(b + (uint64_t)kC * sz + kC, scale4(a10, px));
-        red4(b + (uint64_t)kC * (sz + sy), scale4(a11, dx));
-        red4(b + (uint64_t)kC * (sz + sy) + kC, scale4(a11, px));
+        const uint64_t o = (uint64_t)kC * vb + 4 * q;
+        const uint64_t c[8] = {o, o + kC, o + (uint64_t)kC * sy, o + (uint64_t)kC * sy + kC, o + (uint64_t)kC * sz,
+                               o + (uint64_t)kC * sz + kC, o + (uint64_t)kC * (sz + sy),
+                               o + (uint64_t)kC * (sz + sy) + kC};
+        const float4 v[8] = {scale4(a00, dx), scale4(a00, px), scale4(a01, dx), scale4(a01, px),
+                             scale4(a10, dx), scale4(a10, px), scale4(a11, dx), scale4(a11, px)};
+        if (p.grad_bf16) {
+            __nv_bfloat16 *b = reinterpret_cast<__nv_bfloat16 *>(p.data_grad);
+#pragma unroll
+            for (int t = 0; t < 8; ++t) red4_bf16(b + c[t], v[t]);
+        } else {
+#pragma unroll
+            for (int t = 0; t < 8; ++t) red4(p.data_grad + c[t], v[t]);
+        }
     }
 }
 
@@ -969,6 +986,7 @@ int launch(const qsdvr_render_args *a, cudaStream_t stream) {
     p.sample_alpha = a->sample_alpha;
     p.sample_capacity = a->sample_capacity;
     p.order = a->order;
+    p.grad_bf16 = a->data_grad_storage == QSDVR_STORAGE_BF16;
     unsigned blocks = grid_for(a->ray_count, kWarpsPerBlock);
     if (a->workspace) {
         const Layout L = layout_for(a, kPass);
@@ -1018,6 +1036,8 @@ int validate(const qsdvr_render_args *a, int pass) {
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null grad_color");
     if (pass == kTrain && a->ray_count && (!a->target || !a->loss))
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: null target or loss");
+    if (a->data_grad_storage != QSDVR_STORAGE_F32 && a->data_grad_storage != QSDVR_STORAGE_BF16)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: bad data_grad_storage %d", a->data_grad_storage);
     if (a->workspace && !aligned(a->workspace, 256))
         return set_error(QSDVR_ERR_ALIGNMENT, "render: workspace needs 256-byte alignment");
     return QSDVR_OK;

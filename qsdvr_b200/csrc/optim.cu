@@ -15,7 +15,7 @@ QSDVR_ERROR_WORD_ACCESSOR(optim)
 namespace {
 
 struct AdamParams {
-    float *param, *grad, *m, *v;
+    float *param, *grad, *m, *v;  // grad holds bf16 values in the kBf16Grad kernel
     __nv_bfloat16 *copy;
     uint64_t n;
     float b1, b2, one_minus_b1, one_minus_b2, step_size, bc2_sqrt, eps;
@@ -30,11 +30,31 @@ __device__ __forceinline__ void adam_one(float &p, float g, float &m, float &v, 
     p = p - a.step_size * (m / denom);
 }
 
+// Gradient elements [4i, 4i + 4) as floats, and their zeroing, for fp32 or bf16 gradients.
+template <bool kBf16Grad>
+__device__ __forceinline__ float4 grad4(const AdamParams &a, uint64_t i) {
+    if (!kBf16Grad) return ld4(a.grad + 4 * i);
+    const uint2 r = reinterpret_cast<const uint2 *>(a.grad)[i];
+    return make_float4(__uint_as_float(r.x << 16), __uint_as_float(r.x & 0xffff0000u), __uint_as_float(r.y << 16),
+                       __uint_as_float(r.y & 0xffff0000u));
+}
+template <bool kBf16Grad>
+__device__ __forceinline__ void zero_grad4(const AdamParams &a, uint64_t i) {
+    if (kBf16Grad) reinterpret_cast<uint2 *>(a.grad)[i] = make_uint2(0u, 0u);
+    else st4(a.grad + 4 * i, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+}
+template <bool kBf16Grad>
+__device__ __forceinline__ float grad1(const AdamParams &a, uint64_t i) {
+    if (!kBf16Grad) return a.grad[i];
+    return __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(a.grad)[i]);
+}
+
+template <bool kBf16Grad>
 __global__ void __launch_bounds__(256) adam_kernel(const AdamParams a) {
     const uint64_t n4 = a.n / 4;
     const uint64_t stride = (uint64_t)gridDim.x * 256;
     for (uint64_t i = blockIdx.x * 256ull + threadIdx.x; i < n4; i += stride) {
-        float4 g = ld4(a.grad + 4 * i);
+        float4 g = grad4<kBf16Grad>(a, i);
         if (a.skip_zero && g.x == 0.0f && g.y == 0.0f && g.z == 0.0f && g.w == 0.0f) continue;
         float4 p = ld4(a.param + 4 * i), m = ld4(a.m + 4 * i), v = ld4(a.v + 4 * i);
         if (!a.skip_zero || g.x != 0.0f) adam_one(p.x, g.x, m.x, v.x, a);
@@ -44,7 +64,7 @@ __global__ void __launch_bounds__(256) adam_kernel(const AdamParams a) {
         st4(a.param + 4 * i, p);
         st4(a.m + 4 * i, m);
         st4(a.v + 4 * i, v);
-        if (a.zero_grad) st4(a.grad + 4 * i, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+        if (a.zero_grad) zero_grad4<kBf16Grad>(a, i);
         if (a.copy) {
             __nv_bfloat162 lo = __floats2bfloat162_rn(p.x, p.y), hi = __floats2bfloat162_rn(p.z, p.w);
             uint2 packed;
@@ -55,14 +75,17 @@ __global__ void __launch_bounds__(256) adam_kernel(const AdamParams a) {
     }
     // tail (n not a multiple of 4)
     for (uint64_t i = 4 * n4 + blockIdx.x * 256ull + threadIdx.x; i < a.n; i += stride) {
-        const float g = a.grad[i];
+        const float g = grad1<kBf16Grad>(a, i);
         if (a.skip_zero && g == 0.0f) continue;
         float p = a.param[i], m = a.m[i], v = a.v[i];
         adam_one(p, g, m, v, a);
         a.param[i] = p;
         a.m[i] = m;
         a.v[i] = v;
-        if (a.zero_grad) a.grad[i] = 0.0f;
+        if (a.zero_grad) {
+            if (kBf16Grad) reinterpret_cast<__nv_bfloat16 *>(a.grad)[i] = __float2bfloat16_rn(0.0f);
+            else a.grad[i] = 0.0f;
+        }
         if (a.copy) a.copy[i] = __float2bfloat16_rn(p);
     }
 }
@@ -105,6 +128,7 @@ extern "C" int qsdvr_adam_step(const qsdvr_adam_args *args, cudaStream_t stream)
     unsigned blocks = grid_for(work, 256);
     const unsigned cap = 148u * 16;  // a few waves of resident blocks, grid-stride beyond
     if (blocks > cap) blocks = cap;
-    adam_kernel<<<blocks, 256, 0, stream>>>(a);
+    if (args->flags & QSDVR_ADAM_GRAD_BF16) adam_kernel<true><<<blocks, 256, 0, stream>>>(a);
+    else adam_kernel<false><<<blocks, 256, 0, stream>>>(a);
     return check_launch("qsdvr_adam_step");
 }

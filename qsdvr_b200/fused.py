@@ -33,7 +33,7 @@ class RenderArgs(ctypes.Structure):
                 ("sdf_grid", P), ("data", P), ("color", P), ("target", P), ("grad_color", P), ("sdf_grad", P),
                 ("data_grad", P), ("loss", P), ("grad_scale", F32), ("workspace", P), ("workspace_bytes", ctypes.c_uint64),
                 ("sdf_layers", P), ("sdf_layers_grad", P), ("tlist", P), ("sample_alpha", P),
-                ("sample_capacity", ctypes.c_uint64), ("order", P)]
+                ("sample_capacity", ctypes.c_uint64), ("order", P), ("data_grad_storage", I32)]
 
 
 _lib.extra_signatures({
@@ -135,6 +135,11 @@ def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="
         if sample_alpha.device != dev or sample_alpha.dtype != torch.float32 or not sample_alpha.is_contiguous():
             raise ValueError(f"sample_alpha must be a contiguous float32 tensor on {dev}")
         a.sample_alpha, a.sample_capacity = _ptr(sample_alpha), sample_alpha.numel()
+    if data_grad is not None:
+        if (data_grad.device != dev or data_grad.dtype not in (torch.float32, torch.bfloat16)
+                or data_grad.numel() != data.numel() or not data_grad.is_contiguous()):
+            raise ValueError("data_grad must be a contiguous float32 or bfloat16 tensor shaped like data")
+        a.data_grad_storage = STORAGE["bf16" if data_grad.dtype == torch.bfloat16 else "f32"]
     if order is not None:
         if order.device != dev or order.dtype != torch.int32 or order.shape != (n,) or not order.is_contiguous():
             raise ValueError(f"order must be a contiguous int32 [N] permutation on {dev}")
@@ -184,13 +189,14 @@ def render_forward(rays, origin, direction, sdf_grid, data, reso, interval, k, m
 def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
                     mode="compat", transmittance="product", persistent=True, tlist=None, sdf_layers=None,
                     order=None):
-    """Accumulate dL/d(sdf_grid) and dL/d(data) (fp32) for a given dL/dcolor.  With
-    ``sdf_layers``, ``sdf_grad`` is the tables' gradient ([3R+1,4], see ``separable_grad``)."""
+    """Accumulate dL/d(sdf_grid) (fp32) and dL/d(data) (fp32, or bf16 when ``data_grad`` is a
+    bfloat16 tensor) for a given dL/dcolor.  With ``sdf_layers``, ``sdf_grad`` is the tables'
+    gradient ([3R+1,4], see ``separable_grad``)."""
     dev, n = _check_batch(rays, origin, direction)
     sdf_src = sdf_layers if sdf_layers is not None else sdf_grid
-    for t, nm, shape in ((sdf_grad, "sdf_grad", sdf_src.numel()), (data_grad, "data_grad", data.numel())):
-        if t.dtype != torch.float32 or t.numel() != shape or t.device != dev or not t.is_contiguous():
-            raise ValueError(f"{nm} must be a contiguous float32 tensor shaped like its grid")
+    if (sdf_grad.dtype != torch.float32 or sdf_grad.numel() != sdf_src.numel() or sdf_grad.device != dev
+            or not sdf_grad.is_contiguous()):
+        raise ValueError("sdf_grad must be a contiguous float32 tensor shaped like its grid")
     g = grad_color.contiguous().float()
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, grad_color=g,
                   sdf_grad=None if sdf_layers is not None else sdf_grad, data_grad=data_grad,
@@ -205,7 +211,9 @@ def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval
                  sample_alpha=None, sdf_layers=None, order=None):
     """Forward + MSE (mean over N x 3) + backward in one launch.  Returns (color, loss_sum)
     where loss_sum accumulates sum |color - target|^2 (divide by 3N for the mean).  With
-    ``sdf_layers``, ``sdf_grad`` is the tables' gradient ([3R+1,4])."""
+    ``sdf_layers``, ``sdf_grad`` is the tables' gradient ([3R+1,4]).  A bfloat16 ``data_grad``
+    accumulates the appearance gradient in bf16 (half its traffic; the SDF gradient stays
+    fp32)."""
     dev, n = _check_batch(rays, origin, direction)
     if color is None:
         color = torch.empty((n, 3), dtype=torch.float32, device=dev)

@@ -13,6 +13,7 @@ from ._lib import I32, P, U32, U64, call
 
 ZERO_GRAD = 1
 SKIP_ZERO_GRAD = 2
+GRAD_BF16 = 4
 
 
 class AdamArgs(ctypes.Structure):
@@ -27,9 +28,12 @@ _lib.extra_signatures({"qsdvr_adam_step": [ctypes.POINTER(AdamArgs), P]})
 
 def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, betas=(0.9, 0.999), eps=1e-8, param_bf16=None,
               zero_grad=True, skip_zero_grad=False):
-    for t, nm in ((param, "param"), (grad, "grad"), (exp_avg, "exp_avg"), (exp_avg_sq, "exp_avg_sq")):
+    for t, nm in ((param, "param"), (exp_avg, "exp_avg"), (exp_avg_sq, "exp_avg_sq")):
         if not t.is_cuda or t.dtype != torch.float32 or not t.is_contiguous() or t.numel() != param.numel():
             raise ValueError(f"{nm} must be a contiguous CUDA float32 tensor shaped like param")
+    if (not grad.is_cuda or grad.dtype not in (torch.float32, torch.bfloat16) or not grad.is_contiguous()
+            or grad.numel() != param.numel()):
+        raise ValueError("grad must be a contiguous CUDA float32 or bfloat16 tensor shaped like param")
     if param_bf16 is not None and (param_bf16.dtype != torch.bfloat16 or param_bf16.numel() != param.numel()):
         raise ValueError("param_bf16 must be a bfloat16 tensor shaped like param")
     a = AdamArgs()
@@ -38,7 +42,8 @@ def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, betas=(0.9, 0.999), ep
     a.count = param.numel()
     a.lr, a.beta1, a.beta2, a.eps = float(lr), float(betas[0]), float(betas[1]), float(eps)
     a.step = int(step)
-    a.flags = (ZERO_GRAD if zero_grad else 0) | (SKIP_ZERO_GRAD if skip_zero_grad else 0)
+    a.flags = ((ZERO_GRAD if zero_grad else 0) | (SKIP_ZERO_GRAD if skip_zero_grad else 0)
+               | (GRAD_BF16 if grad.dtype == torch.bfloat16 else 0))
     with torch.cuda.device(param.device):
         call("qsdvr_adam_step", ctypes.byref(a), ctypes.c_void_p(torch.cuda.current_stream(param.device).cuda_stream))
 
@@ -46,12 +51,16 @@ def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, betas=(0.9, 0.999), ep
 class FusedGridAdam(torch.optim.Optimizer):
     """Adam for grid parameters using the fused kernel.  ``step()`` also zeroes the
     gradients (so ``zero_grad()`` is a no-op) and, for parameters registered with a bf16
-    copy via ``bf16_copies={param: copy}``, refreshes the copy."""
+    copy via ``bf16_copies={param: copy}``, refreshes the copy.  ``grads={param: tensor}``
+    names a gradient buffer to use instead of ``param.grad`` (e.g. a bf16 one, which torch
+    does not allow as the .grad of an fp32 parameter)."""
 
-    def __init__(self, params, lr=1e-2, betas=(0.9, 0.999), eps=1e-8, bf16_copies=None, skip_zero_grad=False):
+    def __init__(self, params, lr=1e-2, betas=(0.9, 0.999), eps=1e-8, bf16_copies=None, skip_zero_grad=False,
+                 grads=None):
         super().__init__(params, dict(lr=lr, betas=betas, eps=eps))
         self.bf16_copies = bf16_copies or {}
         self.skip_zero_grad = skip_zero_grad
+        self.grads = grads or {}
 
     def zero_grad(self, set_to_none: bool = False):
         pass  # step() already wrote zeros over the gradients it consumed
@@ -60,7 +69,8 @@ class FusedGridAdam(torch.optim.Optimizer):
     def step(self, closure=None):
         for group in self.param_groups:
             for p in group["params"]:
-                if p.grad is None:
+                grad = self.grads.get(p, p.grad)
+                if grad is None:
                     continue
                 st = self.state[p]
                 if not st:
@@ -68,5 +78,5 @@ class FusedGridAdam(torch.optim.Optimizer):
                     st["exp_avg"] = torch.zeros_like(p, memory_format=torch.contiguous_format)
                     st["exp_avg_sq"] = torch.zeros_like(p, memory_format=torch.contiguous_format)
                 st["step"] += 1
-                adam_step(p.data, p.grad, st["exp_avg"], st["exp_avg_sq"], st["step"], group["lr"], group["betas"],
+                adam_step(p.data, grad, st["exp_avg"], st["exp_avg_sq"], st["step"], group["lr"], group["betas"],
                           group["eps"], self.bf16_copies.get(p), True, self.skip_zero_grad)

@@ -86,6 +86,8 @@ def parser():
     ap.add_argument("--save", default=None, help="checkpoint path written at the end (and every --save-every)")
     ap.add_argument("--save-every", type=int, default=0)
     ap.add_argument("--resume", default=None, help="checkpoint to continue from (steps counts the total)")
+    ap.add_argument("--grad-storage", default="f32", choices=["f32", "bf16"],
+                    help="accumulate the appearance gradient in bf16 (half its traffic; SDF gradient fp32)")
     ap.add_argument("--no-ray-order", dest="ray_order", action="store_false",
                     help="take each batch's rays in batch order instead of the Morton order of their midpoints")
     ap.add_argument("--model", default="dense", choices=["dense", "separable"],
@@ -116,9 +118,14 @@ def run(a, data=None, quiet=False, return_state=False):
     base_mem = torch.cuda.memory_allocated(dev)
     model = fused.DenseRenderGrid(R, a.k, a.interval, mode=a.mode, storage=a.storage, device=dev, sh_degree=a.sh)
     copies = dict(zip((model.sdfGrid, model.renderData), model._copies)) if a.storage == "bf16" else None
-    opt = FusedGridAdam(model.parameters(), lr=a.lr, bf16_copies=copies)
+    data_grad = None
+    if getattr(a, "grad_storage", "f32") == "bf16":
+        data_grad = torch.zeros(model.renderData.shape, dtype=torch.bfloat16, device=dev)
+    opt = FusedGridAdam(model.parameters(), lr=a.lr, bf16_copies=copies,
+                        grads={model.renderData: data_grad} if data_grad is not None else None)
     model.sdfGrid.grad = torch.zeros_like(model.sdfGrid)
-    model.renderData.grad = torch.zeros_like(model.renderData)
+    if data_grad is None:
+        model.renderData.grad = data_grad = torch.zeros_like(model.renderData)
     net = ProposalNet(dev, seed=a.seed, lr=a.proposal_lr) if (a.proposal or a.online_proposal) else None
     first = 1
     if getattr(a, "resume", None):
@@ -159,7 +166,7 @@ def run(a, data=None, quiet=False, return_state=False):
             if a.proposal and step > a.proposal_warmup:
                 tlist = net.sample(r, o, d, a.interval, a.proposal_mix)
         order = fused.ray_order(r, o, d, a.interval) if a.ray_order else None
-        fused.render_train(tg, r, o, d, sg, dg, R, a.interval, a.k, model.sdfGrid.grad, model.renderData.grad,
+        fused.render_train(tg, r, o, d, sg, dg, R, a.interval, a.k, model.sdfGrid.grad, data_grad,
                            a.mode, model.transmittance, loss=loss, tlist=tlist, order=order)
         e1.record()
         opt.step()  # Adam on the fp32 masters; zeroes the gradients, refreshes bf16 copies

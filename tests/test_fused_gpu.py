@@ -293,3 +293,34 @@ def test_ray_order_gives_same_results(fz):
     bad[0] = n + 5
     fz.render_forward(*args, grid8, data, R, interval, k, "fixed", order=bad)
     assert _lib.device_error() & _lib.QSDVR_DEVERR_RAY
+
+
+def test_bf16_data_gradient(fz):
+    """data_grad_storage bf16: the same colours and SDF gradient as with an fp32 data
+    gradient, and the appearance gradient within the rounding of bf16 accumulation (each
+    vertex row receives a few contributions per batch: 2e-2 relative)."""
+    from qsdvr_b200 import _lib, scenes
+
+    R, k, interval = 32, 8.0, 4.0 / 96
+    cam = camera_batch((-2.0, 3.0, 1.6), 56, 75.0, interval, R)
+    grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.55, 0.01, seed=13).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=13).to(DEV)
+    target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(14)).to(DEV)
+    args = (cam.rayList, cam.originList, cam.dirList)
+    res = []
+    for dt in (torch.float32, torch.bfloat16):
+        for storage in ("f32", "bf16"):
+            g = (grid8, data) if storage == "f32" else (grid8.to(torch.bfloat16), data.to(torch.bfloat16))
+            sg, dg = torch.zeros_like(grid8), torch.zeros(data.shape, dtype=dt, device=DEV)
+            col, _ = fz.render_train(target, *args, *g, R, interval, k, sg, dg, mode="fixed",
+                                     transmittance="product" if storage == "f32" else "log")
+            res.append((storage, dt, col, sg, dg))
+    by = {(s, d): (c, sg, dg) for s, d, c, sg, dg in res}
+    for storage in ("f32", "bf16"):
+        c32, s32, d32 = by[(storage, torch.float32)]
+        c16, s16, d16 = by[(storage, torch.bfloat16)]
+        assert torch.equal(c32, c16)
+        assert rel_err(s16.cpu(), s32.cpu()) < 1e-5
+        err = rel_err(d16.float().cpu(), d32.cpu())
+        assert 0 < err < 2e-2, (storage, err)
+    assert _lib.device_error() == 0

@@ -48,3 +48,23 @@ def test_skip_zero_grad_leaves_untouched_entries():
     touched = torch.ones(n, dtype=torch.bool, device=DEV)
     touched[::3] = False
     assert (p[touched] != p0[touched]).all()
+
+
+@pytest.mark.parametrize("n", [4096 * 33 + 3, 1 << 20])
+def test_bf16_gradient_adam_matches_fp32(n):
+    """QSDVR_ADAM_GRAD_BF16: the fused step reads a bf16 gradient exactly as the same values in
+    fp32 (parameters, moments and the bf16 copy identical) and zeroes it."""
+    from qsdvr_b200.optim import adam_step
+
+    gen = torch.Generator(device=DEV).manual_seed(3)
+    p0 = torch.randn(n, generator=gen, device=DEV)
+    g16 = (torch.randn(n, generator=gen, device=DEV) * 0.3).to(torch.bfloat16)
+    outs = []
+    for grad in (g16.clone(), g16.float()):
+        p, m, v = p0.clone(), torch.zeros_like(p0), torch.zeros_like(p0)
+        copy = torch.empty(n, dtype=torch.bfloat16, device=DEV)
+        adam_step(p, grad, m, v, 1, 1e-2, param_bf16=copy)
+        assert torch.count_nonzero(grad) == 0
+        outs.append((p, m, v, copy))
+    for a, b in zip(*outs):
+        assert torch.equal(a, b)
