@@ -40,7 +40,9 @@ enum {
     QSDVR_DEVERR_INDEX = 1u,        /* a cell / vertex index outside the grid         */
     QSDVR_DEVERR_CAPACITY = 2u,     /* a ray's samples run past the sample buffers     */
     QSDVR_DEVERR_RAY = 4u,          /* a ray record is inconsistent (count 1, overflow) */
-    QSDVR_DEVERR_TIMEOUT = 8u       /* a bounded wait on the tensor cores gave up       */
+    QSDVR_DEVERR_TIMEOUT = 8u,      /* a bounded wait on the tensor cores gave up       */
+    QSDVR_DEVERR_BOUNDS = 16u       /* bounds-checked build only: an access outside its
+                                       buffer was caught and redirected                 */
 };
 
 /* Shading / indexing modes.  In the fused renderer, fixed mode also computes alpha and its
@@ -57,6 +59,23 @@ const char *qsdvr_last_error(void);
 int qsdvr_version(void);
 /* Read (and clear when clear != 0) the device error word of the current device. */
 int qsdvr_device_error(uint32_t *word, int clear, cudaStream_t stream);
+
+/* Bounds-checked build (libqsdvr_b200_debug.so, the same sources compiled with
+ * -DQSDVR_DEBUG_BOUNDS; no counterpart in the reference, which checks no index).  Every global
+ * access whose index a kernel derives from geometry or caller data is checked against its
+ * buffer; one outside it sets QSDVR_DEVERR_BOUNDS and is redirected to an in-bounds sink, so
+ * nothing faults.  qsdvr_bounds_checked returns 1 in that build and 0 in the product build.
+ * qsdvr_bounds_record writes the first such access since the last clear as record[0..3] =
+ * {source file (1 camera.cu, 2 surface.cu, 3 render_ops.cu, 4 fused.cu, 5 optim.cu,
+ * 6 gradcheck.cu, 7 proposal.cu), source line, element index, buffer extent in elements},
+ * all zeros when there is none (always in the product build). */
+int qsdvr_bounds_checked(void);
+int qsdvr_bounds_record(uint64_t *record, int clear, cudaStream_t stream);
+/* Positive control of those checks: buffer (device memory) holds 64 floats; one thread writes
+ * 1.0 to element 40 through a check that declares 32 elements.  The bounds-checked build
+ * catches it (QSDVR_DEVERR_BOUNDS, a record {4, line, 40, 32}) and element 40 keeps its value;
+ * the product build writes it.  In bounds either way. */
+int qsdvr_check_bounds(float *buffer, cudaStream_t stream);
 
 /* Check of the failure path of the tensor-core kernels' bounded waits (no counterpart in the
  * reference): one wait, limited to limit_ns (at most 2 s), on an mbarrier that no arrival

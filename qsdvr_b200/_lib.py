@@ -9,7 +9,10 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
+# QSDVR_B200_LIB selects another build of the library, e.g. DEBUG_LIB_PATH, the bounds-checked
+# variant of the same sources (every derived index range-checked; violations recorded).
 LIB_PATH = os.environ.get("QSDVR_B200_LIB") or os.path.join(_HERE, "libqsdvr_b200.so")
+DEBUG_LIB_PATH = os.path.join(_HERE, "libqsdvr_b200_debug.so")
 
 P = ctypes.c_void_p
 U32 = ctypes.c_uint32
@@ -25,6 +28,8 @@ MODE_FIXED = 1
 DEVERR_INDEX = 1
 DEVERR_CAPACITY = 2
 DEVERR_RAY = 4
+DEVERR_TIMEOUT = 8
+DEVERR_BOUNDS = 16
 
 
 class Camera(ctypes.Structure):
@@ -37,6 +42,9 @@ class Camera(ctypes.Structure):
 _SIGS = {
     "qsdvr_version": [],
     "qsdvr_device_error": [P, I32, P],
+    "qsdvr_bounds_checked": [],
+    "qsdvr_bounds_record": [P, I32, P],
+    "qsdvr_check_bounds": [P, P],
     "qsdvr_ray_cut": [ctypes.POINTER(Camera), P, P, P, P, F32, U32, P, P, SZ, P],
     "qsdvr_generate_ray_points": [P, P, P, U32, F32, U32, P, P, P, P, P, U64, U64, P],
     "qsdvr_layer_to_grid_forward": [P, P, P, P, P, U32, P, SZ, P],
@@ -116,6 +124,10 @@ def size(name: str, *args) -> int:
 
 # bits of the device error word (include/qsdvr_b200.h)
 QSDVR_DEVERR_INDEX, QSDVR_DEVERR_CAPACITY, QSDVR_DEVERR_RAY, QSDVR_DEVERR_TIMEOUT = 1, 2, 4, 8
+QSDVR_DEVERR_BOUNDS = 16
+# source files of qsdvr_bounds_record's first field
+BOUNDS_SOURCES = {1: "camera.cu", 2: "surface.cu", 3: "render_ops.cu", 4: "fused.cu", 5: "optim.cu",
+                  6: "gradcheck.cu", 7: "proposal.cu"}
 
 
 def device_error(stream=None, clear: bool = True) -> int:
@@ -123,3 +135,18 @@ def device_error(stream=None, clear: bool = True) -> int:
     w = ctypes.c_uint32(0)
     call("qsdvr_device_error", ctypes.byref(w), int(clear), stream)
     return int(w.value)
+
+
+def bounds_checked() -> bool:
+    """True when the loaded library is the bounds-checked build."""
+    return bool(lib().qsdvr_bounds_checked())
+
+
+def bounds_record(stream=None, clear: bool = True):
+    """The first out-of-range access the bounds-checked build caught since the last clear, as
+    (source file, line, element index, buffer extent), or None; synchronises the stream."""
+    rec = (ctypes.c_uint64 * 4)()
+    call("qsdvr_bounds_record", rec, int(clear), stream)
+    if rec[0] == 0:
+        return None
+    return BOUNDS_SOURCES.get(int(rec[0]), str(int(rec[0]))), int(rec[1]), int(rec[2]), int(rec[3])

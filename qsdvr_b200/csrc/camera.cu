@@ -199,15 +199,15 @@ __global__ void __launch_bounds__(256) generate_points_kernel(
     for (uint32_t j = lane; j < info.sdf_count; j += kWarp) {
         const uint64_t s = (uint64_t)info.sdf_offset + j;
         const CellPoint c = to_cell(march(o, d, (float)j, interval), volume_offset, reso);
-        store3(sdf_points + 3 * s, c.u);
-        sdf_index[s] = c.index;
+        store3(QSDVR_AT(sdf_points, 3 * s, 3, 3 * sdf_cap), c.u);
+        *QSDVR_AT(sdf_index, s, 1, sdf_cap) = c.index;
     }
     for (uint32_t j = lane; j < info.render_count; j += kWarp) {
         const uint64_t s = (uint64_t)info.render_offset + j;
         const CellPoint c = to_cell(midpoint(o, d, j, interval), volume_offset, reso);
-        store3(render_points + 3 * s, c.u);
-        render_index[s] = c.index;
-        store3(view_dir + 3 * s, d);
+        store3(QSDVR_AT(render_points, 3 * s, 3, 3 * render_cap), c.u);
+        *QSDVR_AT(render_index, s, 1, render_cap) = c.index;
+        store3(QSDVR_AT(view_dir, 3 * s, 3, 3 * render_cap), d);
     }
 }
 

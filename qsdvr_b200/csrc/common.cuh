@@ -23,6 +23,74 @@ static __device__ unsigned int g_device_error;
 
 __device__ __forceinline__ void flag_error(unsigned bits) { atomicOr(&g_device_error, bits); }
 
+// ---- bounds-checked build ------------------------------------------------------------------
+// Compiled with -DQSDVR_DEBUG_BOUNDS (libqsdvr_b200_debug.so), every global gather, store and
+// RED whose index a kernel derives from geometry or caller data goes through QSDVR_AT, which
+// checks [index, index + width) against the buffer's extent (all in elements).  A range
+// outside it sets QSDVR_DEVERR_BOUNDS, records the first such (source line, index, extent) of
+// the translation unit and is redirected to a 256-byte sink, so the launch completes and
+// nothing traps.  Without the macro QSDVR_AT is the plain address: the product library's
+// code is unchanged.
+#ifdef QSDVR_DEBUG_BOUNDS
+static __device__ unsigned long long g_bounds_record[3];
+static __device__ __align__(16) unsigned char g_bounds_sink[256];
+
+static __device__ __noinline__ void *bounds_fail(uint64_t index, uint64_t extent, uint32_t line) {
+    flag_error(QSDVR_DEVERR_BOUNDS);
+    if (atomicCAS(&g_bounds_record[0], 0ull, (unsigned long long)line) == 0ull) {
+        g_bounds_record[1] = index;
+        g_bounds_record[2] = extent;
+    }
+    return g_bounds_sink;
+}
+
+// (an access through QSDVR_AT spans at most 256 bytes, the sink's size)
+template <typename T>
+static __device__ __forceinline__ T *checked_at(T *base, uint64_t index, uint64_t width, uint64_t extent, uint32_t line) {
+    if (index < extent && width <= extent - index) return base + index;
+    return static_cast<T *>(bounds_fail(index, extent, line));
+}
+// A wider range (a whole row stash, say) is checked with QSDVR_IN_RANGE, which records a
+// violation the same way and returns false, and the caller skips the access.
+static __device__ __forceinline__ bool checked_range(uint64_t index, uint64_t width, uint64_t extent, uint32_t line) {
+    if (index < extent && width <= extent - index) return true;
+    bounds_fail(index, extent, line);
+    return false;
+}
+#define QSDVR_AT(base, index, width, extent) \
+    ::qsdvr::checked_at((base), (uint64_t)(index), (uint64_t)(width), (uint64_t)(extent), __LINE__)
+#define QSDVR_IN_RANGE(index, width, extent) \
+    ::qsdvr::checked_range((uint64_t)(index), (uint64_t)(width), (uint64_t)(extent), __LINE__)
+#define QSDVR_BOUNDS_CHECKED 1
+#else
+#define QSDVR_AT(base, index, width, extent) ((base) + (index))
+#define QSDVR_IN_RANGE(index, width, extent) true
+#define QSDVR_BOUNDS_CHECKED 0
+#endif
+
+#if QSDVR_BOUNDS_CHECKED
+#define QSDVR_BOUNDS_RECORD_READ(rec, clear, stream, e)                                              \
+    do {                                                                                           \
+        if (e == cudaSuccess) e = cudaMemcpyFromSymbolAsync(rec, g_bounds_record, 3 * sizeof(uint64_t), 0, \
+                                                            cudaMemcpyDeviceToHost, stream);       \
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);                                   \
+        if (e == cudaSuccess && clear && rec[0]) {                                                 \
+            const unsigned long long zero[3] = {0, 0, 0};                                          \
+            e = cudaMemcpyToSymbolAsync(g_bounds_record, zero, sizeof(zero), 0,                    \
+                                        cudaMemcpyHostToDevice, stream);                           \
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);                               \
+        }                                                                                          \
+    } while (0)
+#else
+#define QSDVR_BOUNDS_RECORD_READ(rec, clear, stream, e) \
+    do {                                                \
+        rec[0] = rec[1] = rec[2] = 0;                   \
+    } while (0)
+#endif
+
+// Per translation unit: error_word_<name> reads (and clears) its error word;
+// bounds_record_<name> its first out-of-range record {line, index, extent} (zeros when none
+// or in the product build).
 #define QSDVR_ERROR_WORD_ACCESSOR(name)                                                              \
     cudaError_t error_word_##name(unsigned *word, int clear, cudaStream_t stream) {                \
         unsigned v = 0;                                                                            \
@@ -36,6 +104,11 @@ __device__ __forceinline__ void flag_error(unsigned bits) { atomicOr(&g_device_e
             if (e == cudaSuccess) e = cudaStreamSynchronize(stream);                               \
         }                                                                                          \
         *word |= v;                                                                                \
+        return e;                                                                                  \
+    }                                                                                              \
+    cudaError_t bounds_record_##name(uint64_t *rec, int clear, cudaStream_t stream) {              \
+        cudaError_t e = cudaSuccess;                                                               \
+        QSDVR_BOUNDS_RECORD_READ(rec, clear, stream, e);                                           \
         return e;                                                                                  \
     }
 

@@ -137,27 +137,29 @@ struct Store;
 
 template <>
 struct Store<float> {
-    __device__ static void cell(const void *g, uint32_t c, float *a) {
-        const float *p = static_cast<const float *>(g) + 8ull * c;
+    __device__ static void cell(const void *g, uint32_t c, float *a, uint64_t cells) {
+        const float *p = QSDVR_AT(static_cast<const float *>(g), 8ull * c, 8, 8 * cells);
         const float4 lo = ld4(p), hi = ld4(p + 4);
         a[0] = lo.x; a[1] = lo.y; a[2] = lo.z; a[3] = lo.w;
         a[4] = hi.x; a[5] = hi.y; a[6] = hi.z;
     }
-    __device__ static float4 quad(const void *d, uint32_t v, int q, int C) {
-        return ld4(static_cast<const float *>(d) + (uint64_t)C * v + 4 * q);
+    __device__ static float4 quad(const void *d, uint32_t v, int q, int C, uint64_t verts) {
+        return ld4(QSDVR_AT(static_cast<const float *>(d), (uint64_t)C * v + 4 * q, 4, (uint64_t)C * verts));
     }
 };
 
 template <>
 struct Store<__nv_bfloat16> {
-    __device__ static void cell(const void *g, uint32_t c, float *a) {
-        const uint4 r = *reinterpret_cast<const uint4 *>(static_cast<const __nv_bfloat16 *>(g) + 8ull * c);
+    __device__ static void cell(const void *g, uint32_t c, float *a, uint64_t cells) {
+        const uint4 r =
+            *reinterpret_cast<const uint4 *>(QSDVR_AT(static_cast<const __nv_bfloat16 *>(g), 8ull * c, 8, 8 * cells));
         a[0] = bf_lo(r.x); a[1] = bf_hi(r.x); a[2] = bf_lo(r.y); a[3] = bf_hi(r.y);
         a[4] = bf_lo(r.z); a[5] = bf_hi(r.z); a[6] = bf_lo(r.w);
     }
     // channels [8q, 8q + 8) of vertex v: one 16-byte load (bf16 x 8)
-    __device__ static uint4 oct(const void *d, uint32_t v, int q, int C) {
-        return *reinterpret_cast<const uint4 *>(static_cast<const __nv_bfloat16 *>(d) + (uint64_t)C * v + 8 * q);
+    __device__ static uint4 oct(const void *d, uint32_t v, int q, int C, uint64_t verts) {
+        return *reinterpret_cast<const uint4 *>(
+            QSDVR_AT(static_cast<const __nv_bfloat16 *>(d), (uint64_t)C * v + 8 * q, 8, (uint64_t)C * verts));
     }
 };
 
@@ -173,8 +175,8 @@ struct GatherLanes {
 };
 
 
-__device__ __forceinline__ void red_cell(float *g8, uint32_t cell, const float *g) {
-    float *b = g8 + 8ull * cell;
+__device__ __forceinline__ void red_cell(float *g8, uint32_t cell, const float *g, uint64_t cells) {
+    float *b = QSDVR_AT(g8, 8ull * cell, 8, 8 * cells);
     red4(b, make_float4(g[0], g[1], g[2], g[3]));
     red4(b + 4, make_float4(g[4], g[5], g[6], 0.0f));
 }
@@ -184,7 +186,9 @@ __device__ __forceinline__ void red_cell(float *g8, uint32_t cell, const float *
 // order kernel/surface.cu:3-24 materialises it, so a cell is bit-identical to the dense grid
 // LayerToGrid would write.  The per-axis rows are O(R) and stay in L1/L2.
 __device__ __forceinline__ void sep_cell(const float4 *sep, uint32_t R, const CellPoint &c, float *a) {
-    const float4 x = sep[c.cx], y = sep[R + c.cy], z = sep[2 * R + c.cz];
+    [[maybe_unused]] const uint64_t n = 3ull * R + 1;
+    const float4 x = *QSDVR_AT(sep, c.cx, 1, n), y = *QSDVR_AT(sep, R + c.cy, 1, n),
+                 z = *QSDVR_AT(sep, 2 * R + c.cz, 1, n);
     const float off3 = sep[3 * R].x;
     a[0] = x.x; a[1] = y.x; a[2] = z.x;
     a[3] = x.y; a[4] = y.y; a[5] = z.y;
@@ -194,20 +198,21 @@ __device__ __forceinline__ void sep_cell(const float4 *sep, uint32_t R, const Ce
 // Its adjoint: one 16-byte RED per axis row.  The off3 gradient (the sum of every cell's g6)
 // is recovered from the x rows' g6 sums by the reverse recurrence, so it needs no atomics.
 __device__ __forceinline__ void sep_red(float4 *sg, uint32_t R, const CellPoint &c, const float *g) {
-    red4(reinterpret_cast<float *>(sg + c.cx), make_float4(g[0], g[3], g[6], 0.0f));
-    red4(reinterpret_cast<float *>(sg + R + c.cy), make_float4(g[1], g[4], g[6], 0.0f));
-    red4(reinterpret_cast<float *>(sg + 2 * R + c.cz), make_float4(g[2], g[5], g[6], 0.0f));
+    [[maybe_unused]] const uint64_t n = 3ull * R + 1;
+    red4(reinterpret_cast<float *>(QSDVR_AT(sg, c.cx, 1, n)), make_float4(g[0], g[3], g[6], 0.0f));
+    red4(reinterpret_cast<float *>(QSDVR_AT(sg, R + c.cy, 1, n)), make_float4(g[1], g[4], g[6], 0.0f));
+    red4(reinterpret_cast<float *>(QSDVR_AT(sg, 2 * R + c.cz, 1, n)), make_float4(g[2], g[5], g[6], 0.0f));
 }
 
 template <typename S>
 __device__ __forceinline__ void load_cell(const Params &p, const CellPoint &c, float *a) {
     if (p.sep) sep_cell(p.sep, p.R, c, a);
-    else Store<S>::cell(p.sdf, (uint32_t)c.index, a);
+    else Store<S>::cell(p.sdf, (uint32_t)c.index, a, (uint64_t)p.R * p.R * p.R);
 }
 
 __device__ __forceinline__ void scatter_cell(const Params &p, const CellPoint &c, const float *g) {
     if (p.sep_grad) sep_red(p.sep_grad, p.R, c, g);
-    else red_cell(p.sdf_grad, (uint32_t)c.index, g);
+    else red_cell(p.sdf_grad, (uint32_t)c.index, g, (uint64_t)p.R * p.R * p.R);
 }
 
 __device__ __forceinline__ float4 scale4(float4 v, float w) { return make_float4(v.x * w, v.y * w, v.z * w, v.w * w); }
@@ -366,7 +371,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     const uint32_t i = chunk * kWarp + lane;
     const bool live = i < nr;
     bool ok = live;
-    const float *tl = p.tlist ? p.tlist + (uint64_t)kListT * r : nullptr;
+    const float *tl = p.tlist ? QSDVR_AT(p.tlist, (uint64_t)kListT * r, kListT, (uint64_t)kListT * p.n) : nullptr;
     // SDF sample i+1 (this lane's interval end); sample i comes from the previous lane.
     s.c1 = to_cell(tl ? at_t(o, d, live ? tl[i + 1] : 0.0f) : march(o, d, (float)(i + 1), p.interval),
                    p.volume_offset, R);
@@ -439,6 +444,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
         return;
     }
     const uint32_t sy = R1, sz = R1 * R1;
+    [[maybe_unused]] const uint64_t nv = (uint64_t)R1 * R1 * R1;  // vertex rows
     if constexpr (sizeof(S) == 2) {
         // bf16 storage: groups of kGL lanes fetch one sample's 8 corner rows as 16-byte
         // (bf16 x 8) loads, kGPS samples per step; each lane stages 8 interpolated channels
@@ -454,13 +460,13 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
             const bool gok = __shfl_sync(kFull, s.valid, j);
             float v[8];
             if (gok) {
-                const uint4 v000 = Store<S>::oct(p.data, vb, q8, kC), v001 = Store<S>::oct(p.data, vb + 1, q8, kC);
-                const uint4 v010 = Store<S>::oct(p.data, vb + sy, q8, kC),
-                            v011 = Store<S>::oct(p.data, vb + sy + 1, q8, kC);
-                const uint4 v100 = Store<S>::oct(p.data, vb + sz, q8, kC),
-                            v101 = Store<S>::oct(p.data, vb + sz + 1, q8, kC);
-                const uint4 v110 = Store<S>::oct(p.data, vb + sz + sy, q8, kC),
-                            v111 = Store<S>::oct(p.data, vb + sz + sy + 1, q8, kC);
+                const uint4 v000 = Store<S>::oct(p.data, vb, q8, kC, nv), v001 = Store<S>::oct(p.data, vb + 1, q8, kC, nv);
+                const uint4 v010 = Store<S>::oct(p.data, vb + sy, q8, kC, nv),
+                            v011 = Store<S>::oct(p.data, vb + sy + 1, q8, kC, nv);
+                const uint4 v100 = Store<S>::oct(p.data, vb + sz, q8, kC, nv),
+                            v101 = Store<S>::oct(p.data, vb + sz + 1, q8, kC, nv);
+                const uint4 v110 = Store<S>::oct(p.data, vb + sz + sy, q8, kC, nv),
+                            v111 = Store<S>::oct(p.data, vb + sz + sy + 1, q8, kC, nv);
                 float w[8];
                 corner_weights(gx, gy, gz, w);
                 first_bf8(v000, w[0], v);
@@ -498,13 +504,13 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
         const bool gok = __shfl_sync(kFull, s.valid, j);
         float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (gok) {
-            const float4 v000 = Store<S>::quad(p.data, vb, q, kC), v001 = Store<S>::quad(p.data, vb + 1, q, kC);
-            const float4 v010 = Store<S>::quad(p.data, vb + sy, q, kC),
-                         v011 = Store<S>::quad(p.data, vb + sy + 1, q, kC);
-            const float4 v100 = Store<S>::quad(p.data, vb + sz, q, kC),
-                         v101 = Store<S>::quad(p.data, vb + sz + 1, q, kC);
-            const float4 v110 = Store<S>::quad(p.data, vb + sz + sy, q, kC),
-                         v111 = Store<S>::quad(p.data, vb + sz + sy + 1, q, kC);
+            const float4 v000 = Store<S>::quad(p.data, vb, q, kC, nv), v001 = Store<S>::quad(p.data, vb + 1, q, kC, nv);
+            const float4 v010 = Store<S>::quad(p.data, vb + sy, q, kC, nv),
+                         v011 = Store<S>::quad(p.data, vb + sy + 1, q, kC, nv);
+            const float4 v100 = Store<S>::quad(p.data, vb + sz, q, kC, nv),
+                         v101 = Store<S>::quad(p.data, vb + sz + 1, q, kC, nv);
+            const float4 v110 = Store<S>::quad(p.data, vb + sz + sy, q, kC, nv),
+                         v111 = Store<S>::quad(p.data, vb + sz + sy + 1, q, kC, nv);
             float w[8];
             corner_weights(gx, gy, gz, w);
             v = scale4(v000, w[0]);
@@ -539,7 +545,7 @@ __device__ __forceinline__ void eval_alpha(const Params &p, uint32_t r, f3 o, f3
     const uint32_t i = chunk * kWarp + lane;
     const bool live = i < nr;
     bool ok = live;
-    const float *tl = p.tlist ? p.tlist + (uint64_t)kListT * r : nullptr;
+    const float *tl = p.tlist ? QSDVR_AT(p.tlist, (uint64_t)kListT * r, kListT, (uint64_t)kListT * p.n) : nullptr;
     const CellPoint c1 = to_cell(tl ? at_t(o, d, live ? tl[i + 1] : 0.0f) : march(o, d, (float)(i + 1), p.interval),
                                  p.volume_offset, R);
     float s1 = 0.0f;
@@ -633,6 +639,7 @@ __device__ __forceinline__ void scatter_tile(const Params &p, const float *tile,
     using RW = Rows<kDeg>;
     constexpr int kC = RW::kC, kRow = RW::kStride, kL = RW::kLanes, kPS = RW::kPerStep;
     const uint32_t R1 = p.R + 1, sy = R1, sz = R1 * R1;
+    [[maybe_unused]] const uint64_t ne = (uint64_t)kC * R1 * R1 * R1;  // gradient elements
     const int q = lane % kL;
 #pragma unroll 2
     for (int st = 0; st < kL; ++st) {
@@ -656,10 +663,10 @@ __device__ __forceinline__ void scatter_tile(const Params &p, const float *tile,
         if (p.grad_bf16) {
             __nv_bfloat16 *b = reinterpret_cast<__nv_bfloat16 *>(p.data_grad);
 #pragma unroll
-            for (int t = 0; t < 8; ++t) red4_bf16(b + c[t], v[t]);
+            for (int t = 0; t < 8; ++t) red4_bf16(QSDVR_AT(b, c[t], 4, ne), v[t]);
         } else {
 #pragma unroll
-            for (int t = 0; t < 8; ++t) red4(p.data_grad + c[t], v[t]);
+            for (int t = 0; t < 8; ++t) red4(QSDVR_AT(p.data_grad, c[t], 4, ne), v[t]);
         }
     }
 }
@@ -677,7 +684,11 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
     // balances ray lengths).  With one, the grid is persistent and warps take rays from a
     // counter; in train mode each warp also owns a row stash (slot).
     const bool persistent = p.ray_counter != nullptr;
-    float *slot = (kPass == kTrain && p.slots) ? p.slots + (uint64_t)warp_id * kSlotChunks * kChunkFloats : nullptr;
+    float *slot = (kPass == kTrain && p.slots &&
+                   QSDVR_IN_RANGE((uint64_t)warp_id * kSlotChunks * kChunkFloats, kSlotChunks * kChunkFloats,
+                                  (uint64_t)gridDim.x * kWarpsPerBlock * kSlotChunks * kChunkFloats))
+                      ? p.slots + (uint64_t)warp_id * kSlotChunks * kChunkFloats
+                      : nullptr;
     float sq = 0.0f;
     uint32_t r = persistent ? 0u : warp_id;
     for (;;) {
@@ -689,7 +700,7 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
     if (r >= p.n) break;
     const uint32_t taken = r;  // the ray counter's index; the ray itself may come from an order
     if (p.order) {
-        r = p.order[taken];
+        r = *QSDVR_AT(p.order, taken, 1, p.n);
         if (r >= p.n) {  // not a permutation of the batch: skip the entry
             if (lane == 0) flag_error(QSDVR_DEVERR_RAY);
             if (!persistent) break;
@@ -697,11 +708,12 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
         }
     }
     {
-        const qsdvr_ray_info info = p.rays[r];
+        const qsdvr_ray_info info = *QSDVR_AT(p.rays, r, 1, p.n);
         const uint32_t ns = info.sdf_count;
         const uint32_t nr = ns > 1 ? (p.tlist ? kListT - 1 : ns - 1) : 0;
         const uint32_t chunks = (nr + kWarp - 1) / kWarp;
-        const f3 o = load3(p.origin + 3ull * r), d = load3(p.dir + 3ull * r);
+        const f3 o = load3(QSDVR_AT(p.origin, 3ull * r, 3, 3ull * p.n)),
+                 d = load3(QSDVR_AT(p.dir, 3ull * r, 3, 3ull * p.n));
         f3 C{0.0f, 0.0f, 0.0f};
         bool run = nr > 0;
         if (chunks > kMaxChunks) {
@@ -743,17 +755,17 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                 }
                 C = f3{warp_sum(acc.x), warp_sum(acc.y), warp_sum(acc.z)};
             }
-            if (kPass != kBackward && lane == 0) store3(p.color + 3ull * r, C);
+            if (kPass != kBackward && lane == 0) store3(QSDVR_AT(p.color, 3ull * r, 3, 3ull * p.n), C);
         }
         // ---------------- loss gradient
         f3 g{0.0f, 0.0f, 0.0f};
         if (kPass == kTrain) {
-            const f3 t = load3(p.target + 3ull * r);
+            const f3 t = load3(QSDVR_AT(p.target, 3ull * r, 3, 3ull * p.n));
             const f3 e{C.x - t.x, C.y - t.y, C.z - t.z};
             if (lane == 0) sq += e.x * e.x + e.y * e.y + e.z * e.z;  // C is warp-uniform: count it once
             g = f3{p.grad_scale * e.x, p.grad_scale * e.y, p.grad_scale * e.z};
         } else if (kPass == kBackward) {
-            g = load3(p.grad_color + 3ull * r);
+            g = load3(QSDVR_AT(p.grad_color, 3ull * r, 3, 3ull * p.n));
         }
         // ---------------- backward (chunks in reverse, suffix state carried)
         if (kPass != kForward && run) {
@@ -1079,6 +1091,16 @@ __global__ void __launch_bounds__(256) ray_order_keys_kernel(const qsdvr_ray_inf
     keys[r] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
 }
 
+// Positive control of the bounds-checked build: element kBoundsProbe of a buffer declared to
+// hold kBoundsDeclared elements, which physically holds kBoundsHeld, so the write is in
+// bounds whether or not the check redirects it.
+constexpr uint32_t kBoundsDeclared = 32, kBoundsProbe = 40, kBoundsHeld = 64;
+static_assert(kBoundsDeclared <= kBoundsProbe && kBoundsProbe < kBoundsHeld, "probe inside the held buffer");
+
+__global__ void bounds_check_kernel(float *buf) {
+    *QSDVR_AT(buf, kBoundsProbe, 1, kBoundsDeclared) = 1.0f;
+}
+
 }  // namespace
 }  // namespace qsdvr
 
@@ -1092,6 +1114,12 @@ extern "C" int qsdvr_ray_order_keys(const qsdvr_ray_info *rays, const float *ori
     if (!(interval > 0.0f)) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_order_keys: interval must be > 0");
     ray_order_keys_kernel<<<grid_for(ray_count, 256), 256, 0, stream>>>(rays, origin, dir, ray_count, interval, keys);
     return check_launch("qsdvr_ray_order_keys");
+}
+
+extern "C" int qsdvr_check_bounds(float *buffer, cudaStream_t stream) {
+    if (!buffer) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_check_bounds: null buffer");
+    bounds_check_kernel<<<1, 1, 0, stream>>>(buffer);
+    return check_launch("qsdvr_check_bounds");
 }
 
 extern "C" size_t qsdvr_render_workspace_size(const qsdvr_render_args *args) {

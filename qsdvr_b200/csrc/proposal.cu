@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const float4 *__restrict
     float my_db3 = 0.0f, my_loss = 0.0f;
     for (uint32_t tile = blockIdx.x; tile < tiles && sync.ok; tile += gridDim.x) {
         const uint32_t g = tile * kTile + t;
-        float4 pt = g < P ? pts[g] : make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        float4 pt = g < P ? *QSDVR_AT(pts, g, 1, P) : make_float4(0.0f, 0.0f, 0.0f, -1.0f);
         const bool valid = pt.w >= 0.0f;
         {
             float f[kF];
@@ -416,16 +416,16 @@ struct InferSmem {
 // t = (j + 0.5) L / 64, L = (sdf_count - 1) interval.
 __device__ __forceinline__ f3 infer_input(const float4 *__restrict__ pts, const qsdvr_ray_info *__restrict__ rays,
                                           const float *__restrict__ origin, const float *__restrict__ dir,
-                                          float interval, uint32_t g) {
-    if (rays) {
+                                          float interval, uint32_t g, [[maybe_unused]] uint64_t extent) {
+    if (rays) {  // extent = rays
         const uint32_t r = g >> 6, j = g & 63;
-        const uint32_t ns = rays[r].sdf_count;
+        const uint32_t ns = QSDVR_AT(rays, r, 1, extent)->sdf_count;
         const float L = ns > 1 ? (float)(ns - 1) * interval : 0.0f;
         const float tt = ((float)j + 0.5f) * (L / 64.0f);
-        const f3 o = load3(origin + 3ull * r), d = load3(dir + 3ull * r);
+        const f3 o = load3(QSDVR_AT(origin, 3ull * r, 3, 3 * extent)), d = load3(QSDVR_AT(dir, 3ull * r, 3, 3 * extent));
         return f3{fmaf(d.x, tt, o.x), fmaf(d.y, tt, o.y), fmaf(d.z, tt, o.z)};
     }
-    const float4 q = pts[g];
+    const float4 q = *QSDVR_AT(pts, g, 1, extent);  // extent = points
     return f3{q.x, q.y, q.z};
 }
 
@@ -459,17 +459,18 @@ __global__ void __launch_bounds__(128, 6) mlp_infer_kernel(const float4 *__restr
     const uint32_t tiles = (total + kTile - 1) / kTile;
     uint32_t tile = blockIdx.x;
     uint32_t g = tile * kTile + t;
-    f3 p = g < total ? infer_input(pts, rays, origin, dir, interval, g) : f3{0.0f, 0.0f, 0.0f};
-    bool live = g < total && (!rays || rays[g >> 6].sdf_count > 1);
+    [[maybe_unused]] const uint64_t extent = rays ? nrays : P;
+    f3 p = g < total ? infer_input(pts, rays, origin, dir, interval, g, extent) : f3{0.0f, 0.0f, 0.0f};
+    bool live = g < total && (!rays || QSDVR_AT(rays, g >> 6, 1, nrays)->sdf_count > 1);
     while (tile < tiles && sync.ok) {
         const bool valid = g < total, cur_live = live;
         const uint32_t next = tile + gridDim.x;
         const uint32_t gn = next * kTile + t;
         if (!__syncthreads_or(live)) {
             // every ray of the tile misses the volume: its densities are never used
-            if (valid) out[g] = 0.0f;
-            if (next < tiles && gn < total) p = infer_input(pts, rays, origin, dir, interval, gn);
-            live = next < tiles && gn < total && (!rays || rays[gn >> 6].sdf_count > 1);
+            if (valid) *QSDVR_AT(out, g, 1, total) = 0.0f;
+            if (next < tiles && gn < total) p = infer_input(pts, rays, origin, dir, interval, gn, extent);
+            live = next < tiles && gn < total && (!rays || QSDVR_AT(rays, gn >> 6, 1, nrays)->sdf_count > 1);
             tile = next;
             g = gn;
             continue;
@@ -481,10 +482,10 @@ __global__ void __launch_bounds__(128, 6) mlp_infer_kernel(const float4 *__restr
             for (int q = 0; q < 4; ++q) store_row8(xs, t, q, kSpX, f + 8 * q);
         }
         // the next tile's input is in flight while this tile runs on the tensor cores
-        if (next < tiles && gn < total) p = infer_input(pts, rays, origin, dir, interval, gn);
-        live = next < tiles && gn < total && (!rays || rays[gn >> 6].sdf_count > 1);
+        if (next < tiles && gn < total) p = infer_input(pts, rays, origin, dir, interval, gn, extent);
+        live = next < tiles && gn < total && (!rays || QSDVR_AT(rays, gn >> 6, 1, nrays)->sdf_count > 1);
         const float y = infer_tile(xs, w1s, w2s, tmem, sync, S.w3, b3);
-        if (valid && sync.ok) out[g] = cur_live ? softplus(y) : 0.0f;
+        if (valid && sync.ok) *QSDVR_AT(out, g, 1, total) = cur_live ? softplus(y) : 0.0f;
         tile = next;
         g = gn;
     }
@@ -518,7 +519,8 @@ __global__ void __launch_bounds__(256) proposal_sample_kernel(const qsdvr_ray_in
         L[q] = ns > 1 ? (float)(ns - 1) * interval : 0.0f;
         delta[q] = L[q] / 64.0f;
         // two coarse bins per lane: j = 2 lane, 2 lane + 1
-        const float s0 = have ? dens[64ull * r + 2 * lane] : 0.0f, s1 = have ? dens[64ull * r + 2 * lane + 1] : 0.0f;
+        const float s0 = have ? *QSDVR_AT(dens, 64ull * r + 2 * lane, 2, 64ull * nrays) : 0.0f,
+                    s1 = have ? *QSDVR_AT(dens, 64ull * r + 2 * lane + 1, 1, 64ull * nrays) : 0.0f;
         t0[q] = expf(-fmaxf(s0, 0.0f) * delta[q]);  // 1 - alpha
         t1[q] = expf(-fmaxf(s1, 0.0f) * delta[q]);
     }
@@ -590,8 +592,8 @@ __global__ void __launch_bounds__(256) proposal_sample_kernel(const qsdvr_ray_in
             const float frac = span > 0.0f ? (qk - cdf[lo]) / span : 0.5f;
             tk = fminf(((float)lo + fminf(fmaxf(frac, 0.0f), 1.0f)) * delta[q], L[q]);
         }
-        tlist[33ull * r + lane] = tk;
-        if (lane == 0) tlist[33ull * r + 32] = L[q];
+        *QSDVR_AT(tlist, 33ull * r + lane, 1, 33ull * nrays) = tk;
+        if (lane == 0) *QSDVR_AT(tlist, 33ull * r + 32, 1, 33ull * nrays) = L[q];
     }
 }
 
@@ -629,8 +631,8 @@ __global__ void __launch_bounds__(256) proposal_targets_kernel(const qsdvr_ray_i
     for (uint32_t i = lane; i < info.render_count; i += 32) {
         const uint64_t m = (uint64_t)info.render_offset + i;
         const f3 p = midpoint(o, d, i, interval);
-        const float a = fminf(fmaxf(alpha[m], 0.0f), 1.0f - 1e-6f);
-        pts[m] = make_float4(p.x, p.y, p.z, -log1pf(-a) / interval);
+        const float a = fminf(fmaxf(*QSDVR_AT(alpha, m, 1, capacity), 0.0f), 1.0f - 1e-6f);
+        *QSDVR_AT(pts, m, 1, capacity) = make_float4(p.x, p.y, p.z, -log1pf(-a) / interval);
     }
 }
 
@@ -661,7 +663,7 @@ __global__ void __launch_bounds__(256) proposal_draw_kernel(const qsdvr_ray_info
     uint32_t h = mix32(j * 0x9e3779b9u ^ mix32(seed));
     for (int attempt = 0; attempt < 16; ++attempt) {
         const uint32_t r = (uint32_t)(((uint64_t)h * nrays) >> 32);
-        const qsdvr_ray_info info = rays[r];
+        const qsdvr_ray_info info = *QSDVR_AT(rays, r, 1, nrays);
         h = mix32(h + 0x632be5abu);
         if (info.render_count == 0) continue;
         const uint32_t i = (uint32_t)(((uint64_t)h * info.render_count) >> 32);
@@ -670,8 +672,9 @@ __global__ void __launch_bounds__(256) proposal_draw_kernel(const qsdvr_ray_info
             flag_error(QSDVR_DEVERR_CAPACITY);
             break;
         }
-        const f3 p = midpoint(load3(origin + 3ull * r), load3(dir + 3ull * r), i, interval);
-        const float a = fminf(fmaxf(alpha[m], 0.0f), 1.0f - 1e-6f);
+        const f3 p = midpoint(load3(QSDVR_AT(origin, 3ull * r, 3, 3ull * nrays)),
+                              load3(QSDVR_AT(dir, 3ull * r, 3, 3ull * nrays)), i, interval);
+        const float a = fminf(fmaxf(*QSDVR_AT(alpha, m, 1, capacity), 0.0f), 1.0f - 1e-6f);
         out = make_float4(p.x, p.y, p.z, -log1pf(-a) / interval);
         break;
     }

@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(256) aggregate_forward_kernel(float *__restric
             const bool valid = i < info.render_count;
             float a = 0.0f;
             if (valid) {
-                const float e0 = expf(-k * sdf[info.sdf_offset + i]);
-                const float e1 = expf(-k * sdf[info.sdf_offset + i + 1]);
+                const float e0 = expf(-k * *QSDVR_AT(sdf, (uint64_t)info.sdf_offset + i, 2, sdf_cap));
+                const float e1 = expf(-k * *QSDVR_AT(sdf, (uint64_t)info.sdf_offset + i + 1, 1, sdf_cap));
                 a = fmaxf((e1 - e0) / (1.0f + e1), 0.0f);
             }
             float incl = valid ? 1.0f - a : 1.0f;
@@ -187,9 +187,9 @@ __global__ void __launch_bounds__(256) aggregate_forward_kernel(float *__restric
             f3 c{0.0f, 0.0f, 0.0f};
             if (valid) {
                 const uint64_t m = (uint64_t)info.render_offset + i;
-                alpha_out[m] = a;
-                t_out[m] = T;
-                const f3 v = load3(rgb + 3 * m);
+                *QSDVR_AT(alpha_out, m, 1, render_cap) = a;
+                *QSDVR_AT(t_out, m, 1, render_cap) = T;
+                const f3 v = load3(QSDVR_AT(rgb, 3 * m, 3, 3 * render_cap));
                 c = f3{v.x * a * T, v.y * a * T, v.z * a * T};
             }
             color.x += warp_sum(c.x);
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(256) aggregate_backward_kernel(
     if (info.sdf_count == 0 || !ray_ok(info, sdf_cap, render_cap)) return;
     const uint32_t nr = info.render_count;
     if (nr == 0) {
-        if (lane == 0) sdf_grad[info.sdf_offset] = 0.0f;
+        if (lane == 0) *QSDVR_AT(sdf_grad, info.sdf_offset, 1, sdf_cap) = 0.0f;
         return;
     }
     const f3 g = load3(gout + 3 * r);
@@ -230,11 +230,11 @@ __global__ void __launch_bounds__(256) aggregate_backward_kernel(
         f3 c{0.0f, 0.0f, 0.0f};
         if (valid) {
             const uint64_t m = (uint64_t)info.render_offset + i;
-            a = alpha[m];
-            T = tr[m];
-            c = load3(rgb + 3 * m);
-            e0 = expf(-k * sdf[info.sdf_offset + i]);
-            e1 = expf(-k * sdf[info.sdf_offset + i + 1]);
+            a = *QSDVR_AT(alpha, m, 1, render_cap);
+            T = *QSDVR_AT(tr, m, 1, render_cap);
+            c = load3(QSDVR_AT(rgb, 3 * m, 3, 3 * render_cap));
+            e0 = expf(-k * *QSDVR_AT(sdf, (uint64_t)info.sdf_offset + i, 2, sdf_cap));
+            e1 = expf(-k * *QSDVR_AT(sdf, (uint64_t)info.sdf_offset + i + 1, 1, sdf_cap));
         }
         const f3 v{T * a * c.x, T * a * c.y, T * a * c.z};
         // inclusive suffix sum within the chunk
@@ -263,15 +263,17 @@ __global__ void __launch_bounds__(256) aggregate_backward_kernel(
             }
             const f3 dc{T * c.x + after.x / (a - 1), T * c.y + after.y / (a - 1), T * c.z + after.z / (a - 1)};
             dl = g.x * dc.x + g.y * dc.y + g.z * dc.z;
-            store3(rgb_grad + 3 * ((uint64_t)info.render_offset + i), f3{g.x * T * a, g.y * T * a, g.z * T * a});
+            store3(QSDVR_AT(rgb_grad, 3 * ((uint64_t)info.render_offset + i), 3, 3 * render_cap),
+                   f3{g.x * T * a, g.y * T * a, g.z * T * a});
         }
         const float mine_this = dl * d_this;
         float from_next = __shfl_down_sync(kFull, mine_this, 1);
         if (lane == kWarp - 1) from_next = next_this;
         if (valid) {
             // SDF sample i+1 gets this sample's d_next term and the next sample's d_this term.
-            sdf_grad[info.sdf_offset + i + 1] = dl * d_next + (i + 1 < nr ? from_next : 0.0f);
-            if (i == 0) sdf_grad[info.sdf_offset] = mine_this;
+            *QSDVR_AT(sdf_grad, (uint64_t)info.sdf_offset + i + 1, 1, sdf_cap) =
+                dl * d_next + (i + 1 < nr ? from_next : 0.0f);
+            if (i == 0) *QSDVR_AT(sdf_grad, info.sdf_offset, 1, sdf_cap) = mine_this;
         }
         next_this = __shfl_sync(kFull, mine_this, 0);
         tac_carry.x += __shfl_sync(kFull, s.x, 0);

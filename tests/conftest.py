@@ -26,6 +26,22 @@ def pytest_collection_modifyitems(config, items):
             item.add_marker(skip)
 
 
+@pytest.fixture(autouse=True)
+def _no_out_of_range_access():
+    """Under the bounds-checked library (QSDVR_B200_LIB=qsdvr_b200/libqsdvr_b200_debug.so)
+    every test must end with no out-of-range access caught by the kernels' range checks."""
+    yield
+    from qsdvr_b200 import _lib
+
+    if _lib._lib is None or not _lib.bounds_checked():
+        return
+    import torch
+
+    if torch.cuda.is_available():
+        rec = _lib.bounds_record()
+        assert rec is None, f"out-of-range access caught at {rec[0]}:{rec[1]} (index {rec[2]}, extent {rec[3]})"
+
+
 def load_golden(name: str):
     path = os.path.join(GOLDEN, name + ".npz")
     if not os.path.exists(path):

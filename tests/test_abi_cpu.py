@@ -36,6 +36,20 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in declared_functions() if not hasattr(lib, n)]
     assert not missing, missing
     assert lib.qsdvr_version() >= 100
+    assert lib.qsdvr_bounds_checked() == 0  # the product build
+
+
+def test_bounds_checked_build_exports_the_same_symbols():
+    """libqsdvr_b200_debug.so (the same sources with -DQSDVR_DEBUG_BOUNDS) is a drop-in for the
+    product library: the same entry points, and it reports itself as range-checked."""
+    from qsdvr_b200 import _lib
+
+    assert os.path.exists(_lib.DEBUG_LIB_PATH), "build() compiles the bounds-checked library too"
+    dbg = ctypes.CDLL(_lib.DEBUG_LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(dbg, n)]
+    assert not missing, missing
+    assert dbg.qsdvr_bounds_checked() == 1
+    assert dbg.qsdvr_version() == _lib.lib().qsdvr_version()
 
 
 def test_workspace_size_queries():
