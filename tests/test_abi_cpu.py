@@ -37,6 +37,7 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
     assert lib.qsdvr_version() >= 100
     assert lib.qsdvr_bounds_checked() == 0  # the product build
+    assert _lib.bounds_record() is None  # it keeps no record (and needs no GPU to say so)
 
 
 def test_bounds_checked_build_exports_the_same_symbols():
