@@ -332,3 +332,58 @@ def test_bf16_data_gradient(fz):
         err = rel_err(d16.float().cpu(), d32.cpu())
         assert 0 < err < 2e-2, (storage, err)
     assert _lib.device_error() == 0
+
+
+def test_edge_batches(fz):
+    """Edge cases of a batch.
+
+    * An empty batch launches nothing: empty colours, zero loss, gradients untouched.
+    * Rays whose record holds 0 or 1 SDF samples render black and add no gradient.
+    * A ray longer than the 2048 render samples (64 warp chunks) the fused kernels take is
+      skipped before any access and flagged (QSDVR_DEVERR_RAY), rendering black.
+    The other rays of the batch render and train exactly as in a batch without those three."""
+    from qsdvr_b200 import _lib, scenes
+
+    R, k, interval = 32, 8.0, 4.0 / 96
+    cam = camera_batch((1.7, -3.2, 1.3), 48, 65.0, interval, R)
+    grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.55, 0.01, seed=15).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=15).to(DEV)
+    rays, origin, direction = cam.rayList.contiguous(), cam.originList, cam.dirList
+    n = rays.shape[0]
+    target = torch.rand((n, 3), generator=torch.Generator().manual_seed(16)).to(DEV)
+    _lib.device_error()
+
+    # empty batch
+    e4, e3 = rays[:0].contiguous(), origin[:0].contiguous()
+    assert fz.render_forward(e4, e3, e3, grid8, data, R, interval, k, "fixed").shape == (0, 3)
+    sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+    col, loss = fz.render_train(target[:0], e4, e3, e3, grid8, data, R, interval, k, sg, dg, mode="fixed")
+    assert col.shape == (0, 3) and float(loss) == 0.0 and not sg.any() and not dg.any()
+
+    # three rays with samples become: no samples, one sample, too many samples
+    with_samples = torch.nonzero(rays[:, 0] >= 2).reshape(-1).cpu()
+    odd = with_samples[torch.tensor([0, len(with_samples) // 2, len(with_samples) - 1])]
+    keep = torch.ones(n, dtype=torch.bool)
+    keep[odd] = False
+    mod = rays.clone()
+    mod[odd, 0] = torch.tensor([0, 1, 2100], dtype=torch.int32, device=DEV)
+
+    def train(r, o, d, t):
+        sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+        col, loss = fz.render_train(t, r, o, d, grid8, data, R, interval, k, sg, dg, mode="fixed")
+        return col, float(loss), sg, dg
+
+    kd = keep.to(DEV)
+    c0, l0, s0, d0 = train(rays[kd].contiguous(), origin[kd].contiguous(), direction[kd].contiguous(),
+                           target[kd].contiguous())
+    assert _lib.device_error() == 0
+    c1, l1, s1, d1 = train(mod, origin, direction, target)
+    err = _lib.device_error()
+    assert err & _lib.QSDVR_DEVERR_RAY and not err & _lib.QSDVR_DEVERR_INDEX
+    assert float(c1[odd.to(DEV)].abs().max()) == 0.0
+    assert (c1[kd] - c0).abs().max().item() < 1e-6
+    extra = float((target[odd.to(DEV)] ** 2).sum())  # the black rays' squared error
+    assert abs(l1 - (l0 + extra)) <= n * 2.0 ** -24 * max(1.0, l1)
+    # the gradient scale is 2 / (3 N): the same rays' gradients with N = n and N = n - 3
+    scale = (n - 3) / n
+    assert rel_err(s1.cpu(), (s0 * scale).cpu()) < 1e-5 and rel_err(d1.cpu(), (d0 * scale).cpu()) < 1e-5
