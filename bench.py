@@ -69,14 +69,23 @@ WORKLOADS = {
 PROPOSAL_STEPS = 300  # training steps per method in the default line's proposal comparison
 
 
-def bytes_per_sample(storage: str, sh: int, grad: str = "f32") -> int:
-    """Algorithmic bytes per render sample (3-pass model): forward gather 8 C b, backward
-    re-gather 8 C b, gradient scatter 8 C g, quadric cells 192 (C channels, b storage bytes,
-    g gradient bytes)."""
+def byte_terms(storage: str, sh: int, grad: str = "f32") -> tuple[int, int]:
+    """Algorithmic bytes of the train kernel: (per render sample, per active sample).  Every
+    sample gathers its 8 corner rows once (8 C b; the backward rereads them from the warp's
+    L2 stash) and its two quadric cells with their gradient (192).  An active sample, one
+    whose appearance gradient is not zero (alpha > 0), also read-modify-writes its 8
+    gradient rows in L2 (2 x 8 C g); an inactive one sends no RED.  C channels, b storage
+    bytes, g gradient bytes."""
     c = 32 if sh == 2 else 64
     b = 4 if storage == "f32" else 2
     g = 4 if grad == "f32" else 2
-    return 8 * c * b * 2 + 8 * c * g + 192
+    return 8 * c * b + 192, 2 * 8 * c * g
+
+
+def bytes_per_sample(storage: str, sh: int, grad: str = "f32", active: float = 1.0) -> float:
+    """Algorithmic bytes per render sample when a fraction ``active`` of them is active."""
+    every, per_active = byte_terms(storage, sh, grad)
+    return every + active * per_active
 BYTES_PER_RAY = 64  # origin + dir in, target in, colour out, RayInfo
 K_LOGISTIC = 5.0
 METRIC = "train rays/s fwd+bwd @256^3 grid (256 samples/ray, 65536-ray batches)"
@@ -244,6 +253,22 @@ def samples_of(batch):
     return int(torch.clamp(c - 1, min=0).sum())
 
 
+def active_samples_of(batch, sdf_k, data_k, R, interval, mode, transmittance):
+    """Render samples of the batch with alpha > 0 under the model (outside any timed region):
+    one forward of the library with its per-sample alpha output, the ray records given packed
+    render offsets (the fused kernels read only sdf_count besides)."""
+    from qsdvr_b200 import fused
+
+    rays = batch["rays"].clone()
+    cnt = torch.clamp(rays[:, 0].long() - 1, min=0)
+    rays[:, 2] = cnt.to(torch.int32)
+    rays[:, 3] = (torch.cumsum(cnt, 0) - cnt).to(torch.int32)
+    alpha = torch.zeros(int(cnt.sum()), dtype=torch.float32, device=rays.device)
+    fused.render_forward(rays, batch["origin"], batch["dir"], sdf_k, data_k, R, interval, K_LOGISTIC, mode,
+                         transmittance, sample_alpha=alpha)
+    return int((alpha > 0).sum())
+
+
 # ----------------------------------------------------------------------------- timing
 
 def time_device(step, steps, warmup, stream, clock=None, on_start=None):
@@ -316,6 +341,10 @@ def run_ours(args, cfg, device, ws, rank):
         total_ms, kern_ms = time_device(step, args.steps, args.warmup, stream, clk)
     if ws > 1:
         torch.distributed.barrier()
+    # samples with a non-zero appearance gradient under the model the timed region used (the
+    # full-step timing below updates the model)
+    active = [active_samples_of(b, sdf_k, data_k, R, cfg["interval"], mode, transmittance) for b in batches]
+    active_frac = sum(active) / max(1, sum(samples_of(b) for b in batches))
     # ---- e2e through the public API with host buffers (pinned), copies inside the region
     host = []
     for b in batches:
@@ -365,7 +394,7 @@ def run_ours(args, cfg, device, ws, rank):
     # ---- roofline of the train kernel
     samples = [samples_of(b) for b in batches]
     mean_samples = sum(samples) / len(samples)
-    bps = bytes_per_sample(storage, cfg.get("sh", 2), cfg.get("grad", "f32"))
+    bps = bytes_per_sample(storage, cfg.get("sh", 2), cfg.get("grad", "f32"), active_frac)
     alg_bytes = mean_samples * bps + cfg["rays"] * BYTES_PER_RAY
     achieved = alg_bytes / (kern_avg / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
@@ -396,7 +425,8 @@ def run_ours(args, cfg, device, ws, rank):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None if traffic is None else round(traffic),
                      "kernel": "render_kernel<train>", "kernel_ms": round(kern_avg, 4),
-                     "algorithmic_bytes": round(alg_bytes), "bytes_per_sample": bps,
+                     "algorithmic_bytes": round(alg_bytes), "bytes_per_sample": round(bps, 1),
+                     "active_sample_fraction": round(active_frac, 4),
                      "peak_kind": peak_kind},
         "clocks": clk.summary(),
     }

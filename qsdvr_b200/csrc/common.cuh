@@ -130,6 +130,14 @@ __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<floa
 // 16-byte vector reduction into global memory (returns nothing, so it lowers to a RED).
 __device__ __forceinline__ void red4(float *p, float4 v) { atomicAdd(reinterpret_cast<float4 *>(p), v); }
 
+// True when all four values are +0 or -0.  Adding such a vector to a gradient accumulator
+// that starts at +0 changes no bit of it (x + 0 = x for x != 0; +0 + -0 = +0 in round to
+// nearest, so the accumulator never holds -0), and NaN or inf never compares equal to 0, so
+// skipping the RED of a zero vector leaves the sum exactly as it was.
+__device__ __forceinline__ bool is_zero4(float4 v) {
+    return v.x == 0.0f && v.y == 0.0f && v.z == 0.0f && v.w == 0.0f;
+}
+
 inline unsigned grid_for(uint64_t threads, unsigned block) {
     uint64_t g = (threads + block - 1) / block;
     return g == 0 ? 1u : (unsigned)(g > 0x7fffffffull ? 0x7fffffffull : g);

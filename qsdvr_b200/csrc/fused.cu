@@ -177,8 +177,10 @@ struct GatherLanes {
 
 __device__ __forceinline__ void red_cell(float *g8, uint32_t cell, const float *g, uint64_t cells) {
     float *b = QSDVR_AT(g8, 8ull * cell, 8, 8 * cells);
-    red4(b, make_float4(g[0], g[1], g[2], g[3]));
-    red4(b + 4, make_float4(g[4], g[5], g[6], 0.0f));
+    const float4 lo = make_float4(g[0], g[1], g[2], g[3]), hi = make_float4(g[4], g[5], g[6], 0.0f);
+    // a zero half (e.g. a sample whose SDF gradient vanishes with its alpha) is not sent
+    if (!is_zero4(lo)) red4(b, lo);
+    if (!is_zero4(hi)) red4(b + 4, hi);
 }
 
 // Separable SDF (models/render.py:172-207): cell (x, y, z) has coefficients
@@ -199,9 +201,11 @@ __device__ __forceinline__ void sep_cell(const float4 *sep, uint32_t R, const Ce
 // is recovered from the x rows' g6 sums by the reverse recurrence, so it needs no atomics.
 __device__ __forceinline__ void sep_red(float4 *sg, uint32_t R, const CellPoint &c, const float *g) {
     [[maybe_unused]] const uint64_t n = 3ull * R + 1;
-    red4(reinterpret_cast<float *>(QSDVR_AT(sg, c.cx, 1, n)), make_float4(g[0], g[3], g[6], 0.0f));
-    red4(reinterpret_cast<float *>(QSDVR_AT(sg, R + c.cy, 1, n)), make_float4(g[1], g[4], g[6], 0.0f));
-    red4(reinterpret_cast<float *>(QSDVR_AT(sg, 2 * R + c.cz, 1, n)), make_float4(g[2], g[5], g[6], 0.0f));
+    const float4 x = make_float4(g[0], g[3], g[6], 0.0f), y = make_float4(g[1], g[4], g[6], 0.0f),
+                 z = make_float4(g[2], g[5], g[6], 0.0f);
+    if (!is_zero4(x)) red4(reinterpret_cast<float *>(QSDVR_AT(sg, c.cx, 1, n)), x);
+    if (!is_zero4(y)) red4(reinterpret_cast<float *>(QSDVR_AT(sg, R + c.cy, 1, n)), y);
+    if (!is_zero4(z)) red4(reinterpret_cast<float *>(QSDVR_AT(sg, 2 * R + c.cz, 1, n)), z);
 }
 
 template <typename S>
@@ -650,6 +654,11 @@ __device__ __forceinline__ void scatter_tile(const Params &p, const float *tile,
         const bool ok = __shfl_sync(kFull, s.valid, j);
         if (!ok) continue;
         const float4 g = ld4(tile + j * kRow + 4 * q);
+        // A sample with alpha = 0 (the SDF does not fall across its interval) or T = 0 has a
+        // zero appearance gradient, as do channels its shader never reads: its 8 REDs would
+        // add zeros, yet each costs an L2 read-modify-write of a row that is usually not
+        // cached.  Skipped; the sums stay bit-identical (is_zero4).
+        if (is_zero4(g)) continue;
         // kernel/render.cu:136-151
         const float dx = 1 - px, dy = 1 - py;
         const float4 a0 = scale4(g, 1 - pz), a1 = scale4(g, pz);

@@ -68,6 +68,9 @@ __global__ void __launch_bounds__(256) interp_backward_kernel(float *__restrict_
     const float px = (pts[3 * s] + 1.0f) / 2.0f, py = (pts[3 * s + 1] + 1.0f) / 2.0f,
                 pz = (pts[3 * s + 2] + 1.0f) / 2.0f;
     const float4 g = ld4(gout + s * kC + 4 * q);
+    // a zero gradient quad (a sample with alpha = 0 or T = 0) adds nothing: its eight REDs,
+    // each an L2 read-modify-write, are skipped and the sums stay bit-identical (is_zero4)
+    if (is_zero4(g)) return;
     const float dx = 1 - px, dy = 1 - py;
     // kernel/render.cu:136-151: weights applied in the reference's order.
     auto scale = [](float4 v, float w) { return make_float4(v.x * w, v.y * w, v.z * w, v.w * w); };

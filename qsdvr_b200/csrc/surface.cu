@@ -225,6 +225,12 @@ __device__ __forceinline__ bool cell_ok(int32_t idx, uint64_t cells) {
     return true;
 }
 
+// Scalar gradient accumulation that sends no atomic for an exact zero (bit-identical: the
+// accumulator starts at +0 and never holds -0; NaN and inf are still added).
+__device__ __forceinline__ void add_nonzero(float *p, float v) {
+    if (v != 0.0f) atomicAdd(p, v);
+}
+
 // kernel/surface.cu:54-72.
 __global__ void __launch_bounds__(256) sdf_forward_kernel(float *__restrict__ out, const float *__restrict__ g,
                                                           const float *__restrict__ pts,
@@ -266,13 +272,13 @@ __global__ void __launch_bounds__(256) sdf_backward_kernel(const float *__restri
     const float norm = 1.0f / sqrtf(nx * nx + ny * ny + nz * nz);
     const float norm3 = value * norm * norm * norm;
     const float go = gout[id] / reso;
-    atomicAdd(d + 0, go * px * (px * norm - 2 * nx * norm3));
-    atomicAdd(d + 1, go * py * (py * norm - 2 * ny * norm3));
-    atomicAdd(d + 2, go * pz * (pz * norm - 2 * nz * norm3));
-    atomicAdd(d + 3, go * (px * norm - nx * norm3));
-    atomicAdd(d + 4, go * (py * norm - ny * norm3));
-    atomicAdd(d + 5, go * (pz * norm - nz * norm3));
-    atomicAdd(d + 6, go * norm);
+    add_nonzero(d + 0, go * px * (px * norm - 2 * nx * norm3));
+    add_nonzero(d + 1, go * py * (py * norm - 2 * ny * norm3));
+    add_nonzero(d + 2, go * pz * (pz * norm - 2 * nz * norm3));
+    add_nonzero(d + 3, go * (px * norm - nx * norm3));
+    add_nonzero(d + 4, go * (py * norm - ny * norm3));
+    add_nonzero(d + 5, go * (pz * norm - nz * norm3));
+    add_nonzero(d + 6, go * norm);
 }
 
 // kernel/surface.cu:104-115.
@@ -316,12 +322,12 @@ __global__ void __launch_bounds__(256) normal_backward_kernel(const float *__res
     const float gx = ox * (norm - norm3 * vx * vx) - oy * vy * norm3 * vx - oz * vz * norm3 * vx;
     const float gy = oy * (norm - norm3 * vy * vy) - ox * vx * norm3 * vy - oz * vz * norm3 * vy;
     const float gz = oz * (norm - norm3 * vz * vz) - oy * vy * norm3 * vz - ox * vx * norm3 * vz;
-    atomicAdd(d + 0, 2.0f * px * gx);
-    atomicAdd(d + 1, 2.0f * py * gy);
-    atomicAdd(d + 2, 2.0f * pz * gz);
-    atomicAdd(d + 3, gx);
-    atomicAdd(d + 4, gy);
-    atomicAdd(d + 5, gz);
+    add_nonzero(d + 0, 2.0f * px * gx);
+    add_nonzero(d + 1, 2.0f * py * gy);
+    add_nonzero(d + 2, 2.0f * pz * gz);
+    add_nonzero(d + 3, gx);
+    add_nonzero(d + 4, gy);
+    add_nonzero(d + 5, gz);
 }
 
 }  // namespace
