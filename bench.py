@@ -71,15 +71,15 @@ PROPOSAL_STEPS = 300  # training steps per method in the default line's proposal
 
 def byte_terms(storage: str, sh: int, grad: str = "f32") -> tuple[int, int]:
     """Algorithmic bytes of the train kernel: (per render sample, per active sample).  Every
-    sample gathers its 8 corner rows once (8 C b; the backward rereads them from the warp's
-    L2 stash) and its two quadric cells with their gradient (192).  An active sample, one
-    whose appearance gradient is not zero (alpha > 0), also read-modify-writes its 8
-    gradient rows in L2 (2 x 8 C g); an inactive one sends no RED.  C channels, b storage
-    bytes, g gradient bytes."""
+    sample reads its two quadric cells and sends their gradient (192).  An active sample,
+    one with alpha > 0, also gathers its 8 corner rows once (8 C b; the backward rereads
+    them from the warp's L2 stash) and read-modify-writes its 8 gradient rows in L2
+    (2 x 8 C g).  An inactive sample contributes nothing to the colour: its rows are
+    neither gathered nor sent.  C channels, b storage bytes, g gradient bytes."""
     c = 32 if sh == 2 else 64
     b = 4 if storage == "f32" else 2
     g = 4 if grad == "f32" else 2
-    return 8 * c * b + 192, 2 * 8 * c * g
+    return 192, 8 * c * b + 2 * 8 * c * g
 
 
 def bytes_per_sample(storage: str, sh: int, grad: str = "f32", active: float = 1.0) -> float:

@@ -353,6 +353,7 @@ __device__ __forceinline__ void sample_normal_grad(const float *a, f3 u, f3 gn, 
 // Per-lane state of one render sample of a chunk.
 struct Sample {
     bool valid;      // sample exists and all its cells are inside the grid
+    bool shaded;     // valid and its colour matters: its row is gathered and shaded
     float alpha;
     float e0, e1;    // alpha_term of sdf_i and sdf_{i+1}
     f3 rgb, spec, nrm;
@@ -422,6 +423,13 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     s.e0 = alpha_term<kCompat>(p.k, s0);
     s.e1 = alpha_term<kCompat>(p.k, s1);
     s.alpha = ok ? interval_alpha<kCompat>(s.e0, s.e1) : 0.0f;
+    // A valid sample with alpha = 0 (the SDF does not fall across its interval: about half
+    // of a ray's samples) adds alpha T c = 0 to the colour, and every backward term of its
+    // colour is a product with alpha or with dalpha/dsdf, both 0 there.  Its row is neither
+    // gathered nor shaded (rgb = 0), which leaves every output bit-identical for finite
+    // appearance rows.  A non-finite normal keeps the full path, so the NaN colour of a
+    // degenerate cell propagates as in the reference.
+    s.shaded = ok && (s.alpha != 0.0f || !(isfinite(s.nrm.x) && isfinite(s.nrm.y) && isfinite(s.nrm.z)));
     // trilinear weights and base vertex (kernel/render.cu:107-111)
     s.wx = (s.cr.u.x + 1.0f) / 2.0f;
     s.wy = (s.cr.u.y + 1.0f) / 2.0f;
@@ -439,7 +447,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
             st4(tile + j * kRow + 4 * q, ld4_keep(from_slot + j * kC + 4 * q, pol));
         }
         __syncwarp();
-        if (s.valid) {
+        if (s.shaded) {
             s.rgb = shade_any<kCompat, kDeg>(s.nrm, d, tile + lane * kRow, &s.spec);
         } else {
             s.rgb = f3{0.0f, 0.0f, 0.0f};
@@ -461,7 +469,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
             const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
             const float gx = __shfl_sync(kFull, s.wx, j), gy = __shfl_sync(kFull, s.wy, j),
                         gz = __shfl_sync(kFull, s.wz, j);
-            const bool gok = __shfl_sync(kFull, s.valid, j);
+            const bool gok = __shfl_sync(kFull, s.shaded, j);
             float v[8];
             if (gok) {
                 const uint4 v000 = Store<S>::oct(p.data, vb, q8, kC, nv), v001 = Store<S>::oct(p.data, vb + 1, q8, kC, nv);
@@ -505,7 +513,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
         const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
         const float gx = __shfl_sync(kFull, s.wx, j), gy = __shfl_sync(kFull, s.wy, j),
                     gz = __shfl_sync(kFull, s.wz, j);
-        const bool gok = __shfl_sync(kFull, s.valid, j);
+        const bool gok = __shfl_sync(kFull, s.shaded, j);
         float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (gok) {
             const float4 v000 = Store<S>::quad(p.data, vb, q, kC, nv), v001 = Store<S>::quad(p.data, vb + 1, q, kC, nv);
@@ -531,7 +539,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     }
     }
     __syncwarp();
-    if (s.valid) {
+    if (s.shaded) {
         // the row stays in shared memory; the shader reads the channels it needs from it
         s.rgb = shade_any<kCompat, kDeg>(s.nrm, d, tile + lane * kRow, &s.spec);
     } else {
@@ -860,21 +868,28 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                     float a1[7], gq[7];
                     load_cell<S>(p, s.c1, a1);
                     quad_sdf_grad(a1, s.c1.u, (float)p.R, gs1, gq);
-                    // rgb gradient -> shader backward (data gradient into the tile, normal gradient)
-                    const f3 grgb{g.x * T * a, g.y * T * a, g.z * T * a};
-                    // data gradient written over the data row (every read precedes its write)
-                    const f3 gn = shade_any_backward_inplace<kCompat, kDeg>(grgb, s.nrm, d, tile + lane * kRow, s.spec);
-                    float ar[7], gr[6];
-                    load_cell<S>(p, s.cr, ar);
-                    sample_normal_grad<kCompat>(ar, s.cr.u, gn, gr);
-                    if (s.cr.index == s.c1.index) {
+                    if (s.shaded) {
+                        // rgb gradient -> shader backward (data gradient into the tile, normal gradient)
+                        const f3 grgb{g.x * T * a, g.y * T * a, g.z * T * a};
+                        // data gradient written over the data row (every read precedes its write)
+                        const f3 gn =
+                            shade_any_backward_inplace<kCompat, kDeg>(grgb, s.nrm, d, tile + lane * kRow, s.spec);
+                        float ar[7], gr[6];
+                        load_cell<S>(p, s.cr, ar);
+                        sample_normal_grad<kCompat>(ar, s.cr.u, gn, gr);
+                        if (s.cr.index == s.c1.index) {
 #pragma unroll
-                        for (int t = 0; t < 6; ++t) gq[t] += gr[t];
-                        scatter_cell(p, s.c1, gq);
+                            for (int t = 0; t < 6; ++t) gq[t] += gr[t];
+                            scatter_cell(p, s.c1, gq);
+                        } else {
+                            scatter_cell(p, s.c1, gq);
+                            const float g7[7] = {gr[0], gr[1], gr[2], gr[3], gr[4], gr[5], 0.0f};
+                            scatter_cell(p, s.cr, g7);
+                        }
                     } else {
+                        // alpha = 0: the colour's gradients (data row, normal) are 0 and the row
+                        // in the tile is the gather's zeros, which the scatter skips
                         scatter_cell(p, s.c1, gq);
-                        const float g7[7] = {gr[0], gr[1], gr[2], gr[3], gr[4], gr[5], 0.0f};
-                        scatter_cell(p, s.cr, g7);
                     }
                     if (i == 0) {
                         const CellPoint c0 = to_cell(march(o, d, 0.0f, p.interval), p.volume_offset, p.R);
