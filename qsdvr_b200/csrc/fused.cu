@@ -868,9 +868,13 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                     float a1[7], gq[7];
                     load_cell<S>(p, s.c1, a1);
                     quad_sdf_grad(a1, s.c1.u, (float)p.R, gs1, gq);
-                    if (s.shaded) {
+                    // rgb gradient; 0 for an unshaded sample (alpha = 0) unless the ray's colour
+                    // gradient is not finite (a NaN colour), which the reference spreads to
+                    // every sample of the ray: then the unshaded one takes the full path too
+                    // (its zero row gives the same NaN outputs as the real row would)
+                    const f3 grgb{g.x * T * a, g.y * T * a, g.z * T * a};
+                    if (s.shaded || !(isfinite(grgb.x) && isfinite(grgb.y) && isfinite(grgb.z))) {
                         // rgb gradient -> shader backward (data gradient into the tile, normal gradient)
-                        const f3 grgb{g.x * T * a, g.y * T * a, g.z * T * a};
                         // data gradient written over the data row (every read precedes its write)
                         const f3 gn =
                             shade_any_backward_inplace<kCompat, kDeg>(grgb, s.nrm, d, tile + lane * kRow, s.spec);

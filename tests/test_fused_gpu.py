@@ -387,3 +387,40 @@ def test_edge_batches(fz):
     # the gradient scale is 2 / (3 N): the same rays' gradients with N = n and N = n - 3
     scale = (n - 3) / n
     assert rel_err(s1.cpu(), (s0 * scale).cpu()) < 1e-5 and rel_err(d1.cpu(), (d0 * scale).cpu()) < 1e-5
+
+
+def test_nonfinite_colour_propagates_like_the_reference(fz):
+    """compat mode with non-finite values, against the reference build run live.  A cell
+    whose quadric is constant (only a6 != 0) has an infinite SDF and a 0/0 normal.  alpha is
+    0 across such cells, and the reference shades their samples anyway, so the rays crossing
+    them get a NaN colour, and the NaN colour gradient reaches every sample of those rays.
+    The fused kernel skips samples with alpha = 0, unless their normal or rgb gradient is not
+    finite.  So it must give the same NaN rays and the same non-finite gradient entries, and
+    the finite entries within the usual tolerances."""
+    from oracle.build_ref import load_reference
+    from qsdvr_b200 import scenes
+    from tests.golden.make_golden import reference_render
+
+    ref = load_reference()
+    if ref is None:
+        pytest.skip("reference build absent")
+    R, k, interval = 16, 5.0, 4.0 / 64
+    cam = camera_batch((0.3, -4.0, 0.4), 40, 55.0, interval, R)
+    inp = cam.GetRayPoints()
+    g = scenes.sphere_grid(R, 0.5, 0.01, seed=3).reshape(R, R, R, 7).to(DEV)  # [z][y][x]
+    g[4:6] = 0.0
+    g[4:6, :, :, 6] = 0.3  # a slab of constant cells, z in [-0.5, -0.25)
+    grid7 = g.reshape(-1, 7).contiguous()
+    data = scenes.appearance(R, seed=3).to(DEV)
+    target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(4)).to(DEV)
+    want_img, want_g7, want_data = reference_render(ref, grid7, data, inp, R, k, target)
+    nan_rays = ~torch.isfinite(want_img).all(dim=1)
+    assert nan_rays.any() and (~nan_rays).any()  # the case is exercised
+    grid8 = fz.pad_grid7(grid7)
+    sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+    img, _ = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k, sg, dg)
+    assert torch.equal(torch.isfinite(img), torch.isfinite(want_img))
+    fin = torch.isfinite(want_img)
+    assert (img[fin] - want_img[fin]).abs().max().item() < IMG_TOL
+    assert rel_err(sg[:, :7].cpu(), want_g7.cpu()) < GRAD_TOL  # rel_err also requires equal non-finite masks
+    assert rel_err(dg.cpu(), want_data.cpu()) < GRAD_TOL
