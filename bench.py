@@ -308,7 +308,7 @@ def run_ours(args, cfg, device, ws, rank):
     transmittance = "log" if storage == "bf16" else "product"
     mode = "compat" if cfg.get("sh", 2) == 2 else "fixed"
     if storage == "bf16":
-        sdf_k, data_k = sdf.to(torch.bfloat16), data.to(torch.bfloat16)
+        sdf_k, data_k = fused.sdf_cells_bf16(sdf), data.to(torch.bfloat16)
     else:
         sdf_k, data_k = sdf, data
     sg = torch.zeros(sdf.shape, dtype=torch.float32, device=device)
@@ -467,8 +467,8 @@ def full_step_parts(args, cfg, batches, sdf, data, sdf_k, data_k, sg, dg, mode, 
 
     def adam():
         count[0] += 1
-        for q, g, (m, v), c in zip(params, grads, moments, copies):
-            adam_step(q, g, m, v, count[0], 1e-3, param_bf16=c)
+        for j, (q, g, (m, v), c) in enumerate(zip(params, grads, moments, copies)):
+            adam_step(q, g, m, v, count[0], 1e-3, param_bf16=c, sdf_cells=(j == 0))
 
     adam_ms = timed(adam, 5)
 

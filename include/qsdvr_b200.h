@@ -123,10 +123,12 @@ int qsdvr_ray_cut(const qsdvr_camera *camera, const uint8_t *mask, qsdvr_ray_inf
  * and output buffers).  No counterpart in the reference.  Same arguments and results as
  * qsdvr_ray_cut minus the workspace; the scan's scratch is a fixed 128 KiB array in the
  * library's device image, held on every GPU that loads the library until the process
- * exits.  Rejects pixel_count > QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress) with the device
- * current; make that first call before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (other streams, other host threads) race. */
+ * exits.  Rejects pixel_count > QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS.  The first call in each
+ * CUDA context (the device's primary context, a context created after a device reset, or
+ * a host's own driver-API context) looks up that array's device address in the current
+ * context (cudaGetSymbolAddress) and caches it under the context's ID; make that first
+ * call before any stream capture.  All calls share the array: calls that overlap on the GPU
+ * (other streams, other host threads) race. */
 int qsdvr_ray_cut_noalloc(const qsdvr_camera *camera, const uint8_t *mask, qsdvr_ray_info *rays, float *origin,
                           float *dir, float interval, uint32_t pixel_count, uint32_t *totals, cudaStream_t stream);
 
@@ -228,6 +230,7 @@ enum {
  * gradient, QSDVR_DEVERR_RAY set.  The volume's diagonal is 2 sqrt(3), so only intervals
  * below about 0.0017 can produce such a ray (the reference marches any length).
  *   sdf_grid: [R^3][8] (a0..a6 + one pad) in `storage` precision, cell x + yR + zR^2;
+ *             bf16 cells are read as (a0..a5, slot 6 + slot 7), see qsdvr_sdf_cells_bf16;
  *   data:     [(R+1)^3][C] appearance rows in `storage` precision, C = 32 (SH degree 2)
  *             or 64 (degree 3);
  *   grads:    fp32, same layouts, accumulated with atomics (caller zeroes). */
@@ -317,7 +320,9 @@ int qsdvr_render_train(const qsdvr_render_args *args, cudaStream_t stream);
 enum {
     QSDVR_ADAM_ZERO_GRAD = 1,      /* write zeros over the gradient after using it           */
     QSDVR_ADAM_SKIP_ZERO_GRAD = 2, /* leave elements whose gradient is exactly 0 untouched    */
-    QSDVR_ADAM_GRAD_BF16 = 4       /* grad points to bf16 values (render data_grad_storage)  */
+    QSDVR_ADAM_GRAD_BF16 = 4,      /* grad points to bf16 values (render data_grad_storage)  */
+    QSDVR_ADAM_SDF_CELLS = 8       /* param is a quadric cell grid [count/8][8] (fp32 grad): the
+                                      bf16 copy is written in the cell form of qsdvr_sdf_cells_bf16 */
 };
 
 /* One Adam step over `count` fp32 elements.  The default (flags without SKIP_ZERO_GRAD)
@@ -339,6 +344,15 @@ typedef struct qsdvr_adam_args {
 /* Replaces optimizer.step() + optimizer.zero_grad() of the reference's training loop
  * (test.py:34-35, torch.optim.Adam over renderData and the layers) for grid parameters. */
 int qsdvr_adam_step(const qsdvr_adam_args *args, cudaStream_t stream);
+
+/* BF16 storage copy of a quadric cell grid [cell_count][8] fp32 (a0..a6 + pad; no reference
+ * counterpart, the reference keeps fp32 cells).  Each 16-byte bf16 cell holds a0..a5 rounded
+ * to nearest and, in slots 6 and 7, a6' = a6 |bf16(a3..a5)| / |a3..a5| as hi = bf16(a6') and
+ * lo = bf16(a6' - hi): the stored cell's SDF at its centre equals the master's, so rounding
+ * the gradient coefficients does not rescale the cell's SDF.  The render kernels read bf16
+ * cells as (a0..a5, hi + lo); a plain bf16 rounding of the fp32 layout (pad 0) is read as
+ * a6 = bf16(a6). */
+int qsdvr_sdf_cells_bf16(const float *cells, void *out, uint64_t cell_count, cudaStream_t stream);
 
 /* ---- FP64 loss for finite-difference gradient checks ---------------------------------- */
 

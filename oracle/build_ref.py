@@ -20,7 +20,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_ROOT = "/root/reference"
+# where the reference sources lie in this build container; QSDVR_REFERENCE_ROOT or the
+# command-line argument names another tree
+DEFAULT_ROOT = os.environ.get("QSDVR_REFERENCE_ROOT", "/root/reference")
 SOURCES = ("kernel/qsdvr.cpp", "kernel/camera.cu", "kernel/render.cu", "kernel/surface.cu")
 
 

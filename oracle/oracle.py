@@ -215,6 +215,47 @@ def sdf_trusted(grid7: torch.Tensor, points: torch.Tensor, index: torch.Tensor, 
         return torch.isfinite(sdf) & (sdf.abs() <= MAX_SDF) & (len2 >= MIN_GRAD2)
 
 
+def _bf16_bits(x: np.ndarray) -> np.ndarray:
+    """float32 -> bf16 bit patterns, round to nearest even (finite inputs)."""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def _bf16_value(b: np.ndarray) -> np.ndarray:
+    return (b.astype(np.uint32) << 16).view(np.float32)
+
+
+def sdf_cells_bf16(grid8: np.ndarray) -> np.ndarray:
+    """The library's bf16 form of fp32 quadric cells [N,8] (no reference counterpart; the
+    library's qsdvr_sdf_cells_bf16), in float32 numpy with the same rounding steps: a0..a5
+    rounded to nearest, a6' = a6 (|bf16(a3..a5)| / |a3..a5|) split into bf16 hi and lo.
+    Returns the [N,8] uint16 bit patterns."""
+    a = np.ascontiguousarray(grid8, np.float32).reshape(-1, 8)
+    out = np.zeros(a.shape, np.uint16)
+    out[:, :6] = _bf16_bits(a[:, :6])
+    b = _bf16_value(out[:, 3:6])
+    with np.errstate(all="ignore"):
+        n0 = np.sqrt((a[:, 3] * a[:, 3] + a[:, 4] * a[:, 4]) + a[:, 5] * a[:, 5])
+        n1 = np.sqrt((b[:, 0] * b[:, 0] + b[:, 1] * b[:, 1]) + b[:, 2] * b[:, 2])
+        use = (n0 > 0) & np.isfinite(n0) & np.isfinite(n1)
+        c6 = np.where(use, a[:, 6] * np.where(use, n1 / np.where(use, n0, 1), 1), a[:, 6]).astype(np.float32)
+        out[:, 6] = _bf16_bits(c6)
+        lo = (c6 - _bf16_value(out[:, 6])).astype(np.float32)
+        out[:, 7] = np.where(np.isfinite(c6), _bf16_bits(np.where(np.isfinite(lo), lo, 0)), 0)
+    return out
+
+
+def sdf_cells_decode(cells) -> torch.Tensor:
+    """[N,7] float32 coefficients the render kernels read from bf16 cells [N,8] (bit patterns
+    or a torch bfloat16 tensor): a0..a5 and a6 = slot 6 + slot 7."""
+    if torch.is_tensor(cells):
+        cells = cells.detach().cpu().contiguous().view(torch.int16).numpy().view(np.uint16)
+    v = _bf16_value(np.ascontiguousarray(cells, np.uint16).reshape(-1, 8))
+    out = v[:, :7].copy()
+    out[:, 6] = v[:, 6] + v[:, 7]
+    return torch.from_numpy(out)
+
+
 def sample_normal(grid7: torch.Tensor, points: torch.Tensor, index: torch.Tensor):
     """kernel/surface.cu:104-115: normalize(2 a_k u_k + a_{k+3})."""
     g = grid7.reshape(-1, 7)[_t(index).long()]

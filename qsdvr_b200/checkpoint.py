@@ -60,8 +60,7 @@ def load(path, model, optimizer=None, net=None, generator=None) -> int:
         for k, v in state["model"].items():
             params[k].copy_(v)
         if model.storage == "bf16" and model._copies is not None:
-            model._copies[0].copy_(model.sdfGrid.detach())
-            model._copies[1].copy_(model.renderData.detach())
+            model.sync_storage()
     if optimizer is not None:
         if state["optimizer"] is None:
             raise ValueError(f"{path}: the checkpoint holds no optimizer state")

@@ -5,6 +5,10 @@
 // operation uses an explicit round-to-nearest intrinsic in the fused/unfused form the
 // reference's nvcc build (default --fmad=true) evaluates, so no compiler contraction
 // choice can change a count or an index.
+#include <cuda.h>  // CUcontext / CUresult types only; the driver is reached via cudaGetDriverEntryPoint
+
+#include <mutex>
+
 #include "common.cuh"
 #include "raygen.cuh"
 
@@ -275,31 +279,85 @@ namespace {
 
 constexpr uint32_t kStaticScanBlocks = QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS / kScanBlock;
 static_assert(QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS % kScanBlock == 0, "limit must be whole scan blocks");
-constexpr int kMaxDevices = 64;
 
 // One slot per scan block.  Every call overwrites each slot it uses before reading it, so no
 // slot has to start at zero; calls that overlap on the GPU share the array and race.
 static __device__ __align__(256) uint2 g_ray_cut_scratch[kStaticScanBlocks];
 
-// Device address of g_ray_cut_scratch per device.  In host code the symbol name is only a
-// host-side stand-in, so the address is looked up once per device, with that device current.
-uint2 *g_scratch_address[kMaxDevices] = {};
+// Device address of g_ray_cut_scratch per CUDA context.  In host code the symbol name is
+// only a host-side stand-in; the array's device address belongs to the context that loaded
+// the module, so it is looked up (cudaGetSymbolAddress) once per context, with that context
+// current, and cached under the context's ID.  A context ID is never reused within a
+// process: a context created after a device reset, or a host's own driver-API context on
+// the same device, gets its own lookup.  The driver's context queries are reached through
+// cudaGetDriverEntryPoint, so the library does not link libcuda.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+struct ScratchSlot {
+    unsigned long long ctx_id;
+    uint2 *addr;
+};
+constexpr int kScratchSlots = 64;
+std::mutex g_scratch_mutex;
+ScratchSlot g_scratch_slots[kScratchSlots] = {};
+int g_scratch_used = 0, g_scratch_next = 0;
+
+int current_context_id(unsigned long long *id, bool *have) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    static cudaError_t resolved = cudaSuccess;
+    std::call_once(once, [] {
+        void *f = nullptr, *g = nullptr;
+        cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+        resolved = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q1);
+        if (resolved == cudaSuccess) resolved = cudaGetDriverEntryPoint("cuCtxGetId", &g, cudaEnableDefault, &q2);
+        if (resolved == cudaSuccess && q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+            get_id = reinterpret_cast<CtxGetIdFn>(g);
+        }
+    });
+    if (resolved != cudaSuccess) return check_cuda(resolved, "qsdvr_ray_cut_noalloc: cudaGetDriverEntryPoint");
+    if (!get_current || !get_id)
+        return set_error(QSDVR_ERR_UNSUPPORTED, "qsdvr_ray_cut_noalloc: the driver lacks cuCtxGetCurrent/cuCtxGetId");
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS)
+        return set_error(QSDVR_ERR_CUDA, "qsdvr_ray_cut_noalloc: cuCtxGetCurrent failed");
+    *have = ctx != nullptr;
+    if (ctx && get_id(ctx, id) != CUDA_SUCCESS)
+        return set_error(QSDVR_ERR_CUDA, "qsdvr_ray_cut_noalloc: cuCtxGetId failed");
+    return QSDVR_OK;
+}
 
 int scratch_address(uint2 **out) {
-    int dev = 0;
-    int st = check_cuda(cudaGetDevice(&dev), "qsdvr_ray_cut_noalloc: cudaGetDevice");
+    unsigned long long id = 0;
+    bool have = false;
+    int st = current_context_id(&id, &have);
     if (st != QSDVR_OK) return st;
-    if (dev < 0 || dev >= kMaxDevices)
-        return set_error(QSDVR_ERR_UNSUPPORTED, "qsdvr_ray_cut_noalloc: device %d beyond %d", dev, kMaxDevices);
-    uint2 *p = __atomic_load_n(&g_scratch_address[dev], __ATOMIC_ACQUIRE);
-    if (p == nullptr) {
-        void *addr = nullptr;
-        st = check_cuda(cudaGetSymbolAddress(&addr, g_ray_cut_scratch), "qsdvr_ray_cut_noalloc: cudaGetSymbolAddress");
-        if (st != QSDVR_OK) return st;
-        p = static_cast<uint2 *>(addr);
-        __atomic_store_n(&g_scratch_address[dev], p, __ATOMIC_RELEASE);
+    if (have) {
+        std::lock_guard<std::mutex> lock(g_scratch_mutex);
+        for (int i = 0; i < g_scratch_used; ++i)
+            if (g_scratch_slots[i].ctx_id == id) {
+                *out = g_scratch_slots[i].addr;
+                return QSDVR_OK;
+            }
     }
-    *out = p;
+    // First call in this context (or no context yet: the lookup makes the device's primary
+    // context current, and its ID is read afterwards).
+    void *addr = nullptr;
+    st = check_cuda(cudaGetSymbolAddress(&addr, g_ray_cut_scratch), "qsdvr_ray_cut_noalloc: cudaGetSymbolAddress");
+    if (st != QSDVR_OK) return st;
+    if (!have) {
+        st = current_context_id(&id, &have);
+        if (st != QSDVR_OK) return st;
+    }
+    if (have) {
+        std::lock_guard<std::mutex> lock(g_scratch_mutex);
+        const int slot = g_scratch_used < kScratchSlots ? g_scratch_used++ : (g_scratch_next++ % kScratchSlots);
+        g_scratch_slots[slot] = ScratchSlot{id, static_cast<uint2 *>(addr)};
+    }
+    *out = static_cast<uint2 *>(addr);
     return QSDVR_OK;
 }
 

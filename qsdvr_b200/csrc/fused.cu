@@ -154,7 +154,9 @@ struct Store<__nv_bfloat16> {
         const uint4 r =
             *reinterpret_cast<const uint4 *>(QSDVR_AT(static_cast<const __nv_bfloat16 *>(g), 8ull * c, 8, 8 * cells));
         a[0] = bf_lo(r.x); a[1] = bf_hi(r.x); a[2] = bf_lo(r.y); a[3] = bf_hi(r.y);
-        a[4] = bf_lo(r.z); a[5] = bf_hi(r.z); a[6] = bf_lo(r.w);
+        // a6 as the sum of slots 6 and 7 (qsdvr_sdf_cells_bf16: the compensated value split
+        // into two bf16; exact in fp32)
+        a[4] = bf_lo(r.z); a[5] = bf_hi(r.z); a[6] = bf_lo(r.w) + bf_hi(r.w);
     }
     // channels [8q, 8q + 8) of vertex v: one 16-byte load (bf16 x 8)
     __device__ static uint4 oct(const void *d, uint32_t v, int q, int C, uint64_t verts) {

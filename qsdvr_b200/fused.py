@@ -43,6 +43,7 @@ _lib.extra_signatures({
     "qsdvr_separable_sdf_tables": [P, P, P, P, U32, P, P],
     "qsdvr_separable_sdf_grad": [P, U32, P, P, P, P, P],
     "qsdvr_ray_order_keys": [P, P, P, U32, F32, P, P],
+    "qsdvr_sdf_cells_bf16": [P, P, ctypes.c_uint64, P],
 }, {"qsdvr_render_workspace_size": [ctypes.POINTER(RenderArgs)]})
 
 _workspaces: dict = {}
@@ -253,6 +254,23 @@ class FusedRender(autograd.Function):
         return sg.to(sdf_grid.dtype), dg.to(data.dtype), None, None, None, None, None, None, None, None
 
 
+def sdf_cells_bf16(grid8: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """BF16 storage copy [R^3,8] of an fp32 quadric cell grid (qsdvr_sdf_cells_bf16): a0..a5
+    rounded to nearest, a6 rescaled so the stored cell's SDF at its centre equals the
+    master's, held as two bf16 (slots 6 and 7) that the kernels add."""
+    if not grid8.is_cuda or grid8.dtype != torch.float32 or grid8.dim() != 2 or grid8.shape[1] != 8 \
+            or not grid8.is_contiguous():
+        raise ValueError("grid8 must be a contiguous CUDA float32 [cells, 8] tensor")
+    if out is None:
+        out = torch.empty(grid8.shape, dtype=torch.bfloat16, device=grid8.device)
+    elif out.dtype != torch.bfloat16 or out.shape != grid8.shape or out.device != grid8.device \
+            or not out.is_contiguous():
+        raise ValueError("out must be a contiguous bfloat16 tensor shaped like grid8")
+    with torch.cuda.device(grid8.device):
+        call("qsdvr_sdf_cells_bf16", _ptr(grid8), _ptr(out), grid8.shape[0], _stream(grid8.device))
+    return out
+
+
 def pad_grid7(grid7: torch.Tensor) -> torch.Tensor:
     """[R^3,7] (reference layout) -> [R^3,8] (16-byte-aligned rows, a7 = 0)."""
     g = grid7.reshape(-1, 7)
@@ -294,8 +312,21 @@ class DenseRenderGrid(nn.Module):
         self.sync_storage()
 
     def sync_storage(self):
-        if self.storage == "bf16":
-            self._copies = (self.sdfGrid.detach().to(torch.bfloat16), self.renderData.detach().to(torch.bfloat16))
+        """Refresh the bf16 copies from the fp32 masters (in place once they exist, so tensors
+        handed out earlier stay valid).  A model held on the CPU is never rendered (the kernels
+        run on CUDA devices only); its SDF copy is the plain bf16 rounding, which the kernels
+        read the same way, until the model is synced on a GPU."""
+        if self.storage != "bf16":
+            return
+        sdf, data = self.sdfGrid.detach(), self.renderData.detach()
+        if self._copies is None:
+            self._copies = (torch.empty(sdf.shape, dtype=torch.bfloat16, device=sdf.device),
+                            torch.empty(data.shape, dtype=torch.bfloat16, device=data.device))
+        if sdf.is_cuda:
+            sdf_cells_bf16(sdf, out=self._copies[0])
+        else:
+            self._copies[0].copy_(sdf)
+        self._copies[1].copy_(data)
 
     def grids(self):
         if self.storage == "bf16":

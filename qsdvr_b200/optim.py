@@ -14,6 +14,7 @@ from ._lib import I32, P, U32, U64, call
 ZERO_GRAD = 1
 SKIP_ZERO_GRAD = 2
 GRAD_BF16 = 4
+SDF_CELLS = 8
 
 
 class AdamArgs(ctypes.Structure):
@@ -27,7 +28,9 @@ _lib.extra_signatures({"qsdvr_adam_step": [ctypes.POINTER(AdamArgs), P]})
 
 
 def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, betas=(0.9, 0.999), eps=1e-8, param_bf16=None,
-              zero_grad=True, skip_zero_grad=False):
+              zero_grad=True, skip_zero_grad=False, sdf_cells=False):
+    """One fused Adam step.  ``sdf_cells``: ``param`` is a quadric cell grid [R^3,8] and its
+    bf16 copy is written in the compensated cell form (``fused.sdf_cells_bf16``)."""
     for t, nm in ((param, "param"), (exp_avg, "exp_avg"), (exp_avg_sq, "exp_avg_sq")):
         if not t.is_cuda or t.dtype != torch.float32 or not t.is_contiguous() or t.numel() != param.numel():
             raise ValueError(f"{nm} must be a contiguous CUDA float32 tensor shaped like param")
@@ -43,7 +46,7 @@ def adam_step(param, grad, exp_avg, exp_avg_sq, step, lr, betas=(0.9, 0.999), ep
     a.lr, a.beta1, a.beta2, a.eps = float(lr), float(betas[0]), float(betas[1]), float(eps)
     a.step = int(step)
     a.flags = ((ZERO_GRAD if zero_grad else 0) | (SKIP_ZERO_GRAD if skip_zero_grad else 0)
-               | (GRAD_BF16 if grad.dtype == torch.bfloat16 else 0))
+               | (GRAD_BF16 if grad.dtype == torch.bfloat16 else 0) | (SDF_CELLS if sdf_cells else 0))
     with torch.cuda.device(param.device):
         call("qsdvr_adam_step", ctypes.byref(a), ctypes.c_void_p(torch.cuda.current_stream(param.device).cuda_stream))
 
@@ -53,14 +56,16 @@ class FusedGridAdam(torch.optim.Optimizer):
     gradients (so ``zero_grad()`` is a no-op) and, for parameters registered with a bf16
     copy via ``bf16_copies={param: copy}``, refreshes the copy.  ``grads={param: tensor}``
     names a gradient buffer to use instead of ``param.grad`` (e.g. a bf16 one, which torch
-    does not allow as the .grad of an fp32 parameter)."""
+    does not allow as the .grad of an fp32 parameter).  Parameters in ``sdf_cells`` are
+    quadric cell grids [R^3,8]: their bf16 copies take the compensated cell form."""
 
     def __init__(self, params, lr=1e-2, betas=(0.9, 0.999), eps=1e-8, bf16_copies=None, skip_zero_grad=False,
-                 grads=None):
+                 grads=None, sdf_cells=()):
         super().__init__(params, dict(lr=lr, betas=betas, eps=eps))
         self.bf16_copies = bf16_copies or {}
         self.skip_zero_grad = skip_zero_grad
         self.grads = grads or {}
+        self.sdf_cells = {id(p) for p in sdf_cells}
 
     def zero_grad(self, set_to_none: bool = False):
         pass  # step() already wrote zeros over the gradients it consumed
@@ -79,4 +84,5 @@ class FusedGridAdam(torch.optim.Optimizer):
                     st["exp_avg_sq"] = torch.zeros_like(p, memory_format=torch.contiguous_format)
                 st["step"] += 1
                 adam_step(p.data, grad, st["exp_avg"], st["exp_avg_sq"], st["step"], group["lr"], group["betas"],
-                          group["eps"], self.bf16_copies.get(p), True, self.skip_zero_grad)
+                          group["eps"], self.bf16_copies.get(p), True, self.skip_zero_grad,
+                          sdf_cells=id(p) in self.sdf_cells)

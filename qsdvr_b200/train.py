@@ -122,7 +122,8 @@ def run(a, data=None, quiet=False, return_state=False):
     if getattr(a, "grad_storage", "f32") == "bf16":
         data_grad = torch.zeros(model.renderData.shape, dtype=torch.bfloat16, device=dev)
     opt = FusedGridAdam(model.parameters(), lr=a.lr, bf16_copies=copies,
-                        grads={model.renderData: data_grad} if data_grad is not None else None)
+                        grads={model.renderData: data_grad} if data_grad is not None else None,
+                        sdf_cells=(model.sdfGrid,))
     model.sdfGrid.grad = torch.zeros_like(model.sdfGrid)
     if data_grad is None:
         model.renderData.grad = data_grad = torch.zeros_like(model.renderData)

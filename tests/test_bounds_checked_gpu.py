@@ -66,6 +66,7 @@ def test_parity_suites_clean_under_the_checked_build():
     skip = {"test_bounds_checked_gpu.py", "test_reference_speed_gpu.py"}
     files = sorted(f for f in os.listdir(os.path.join(ROOT, "tests"))
                    if f.startswith("test_") and f.endswith("_gpu.py") and f not in skip)
+    files.append("test_zz_no_alloc.py")  # the fixed-scratch RayCut, collected last
     out = _child([sys.executable, "-m", "pytest", *[os.path.join("tests", f) for f in files], "-m", "gpu", "-x", "-q",
                   "-p", "no:cacheprovider"], _lib.DEBUG_LIB_PATH, 1500)
     tail = "\n".join(out.stdout.strip().splitlines()[-15:])

@@ -141,13 +141,14 @@ def test_fused_bf16_storage_vs_oracle(fz):
     cam = camera_batch((-2.5, -2.9, 1.2), 48, 66.0, interval, R)
     grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.5, 0.01, seed=5).reshape(-1, 7)).to(DEV)
     data = scenes.appearance(R, seed=5).to(DEV)
-    g16, d16 = grid8.to(torch.bfloat16), data.to(torch.bfloat16)
+    g16, d16 = fz.sdf_cells_bf16(grid8), data.to(torch.bfloat16)
+    g_read = O.sdf_cells_decode(g16)  # the coefficients the kernels read from the bf16 cells
     target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(6)).to(DEV)
     for mode in ("compat", "fixed"):
         sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
         img, _ = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, g16, d16, R, interval, k, sg, dg,
                                  mode=mode, transmittance="log")
-        want, wg, wd = oracle_render(g16.float(), d16.float(), cam, R, k, compat=(mode == "compat"), target=target)
+        want, wg, wd = oracle_render(g_read, d16.float(), cam, R, k, compat=(mode == "compat"), target=target)
         assert (img.cpu().double() - want).abs().max().item() < IMG_TOL
         assert rel_err(sg[:, :7].cpu(), wg) < GRAD_TOL
         assert rel_err(dg.cpu(), wd) < GRAD_TOL
@@ -238,8 +239,11 @@ def test_fused_sh_degree3_vs_oracle(fz, storage):
     grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.55, 0.01, seed=21).reshape(-1, 7)).to(DEV)
     data = scenes.appearance(R, seed=21, sh_degree=3).to(DEV)
     if storage == "bf16":
-        grid8, data = grid8.to(torch.bfloat16).float(), data.to(torch.bfloat16).float()
-    gk, dk = (grid8.to(torch.bfloat16), data.to(torch.bfloat16)) if storage == "bf16" else (grid8, data)
+        gk, dk = fz.sdf_cells_bf16(grid8), data.to(torch.bfloat16)
+        grid8 = torch.nn.functional.pad(O.sdf_cells_decode(gk), (0, 1)).to(DEV)
+        data = dk.float()
+    else:
+        gk, dk = grid8, data
     target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(22)).to(DEV)
     sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
     img, _ = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, gk, dk, R, interval, k, sg, dg,
@@ -318,7 +322,7 @@ def test_bf16_data_gradient(fz):
     res = []
     for dt in (torch.float32, torch.bfloat16):
         for storage in ("f32", "bf16"):
-            g = (grid8, data) if storage == "f32" else (grid8.to(torch.bfloat16), data.to(torch.bfloat16))
+            g = (grid8, data) if storage == "f32" else (fz.sdf_cells_bf16(grid8), data.to(torch.bfloat16))
             sg, dg = torch.zeros_like(grid8), torch.zeros(data.shape, dtype=dt, device=DEV)
             col, _ = fz.render_train(target, *args, *g, R, interval, k, sg, dg, mode="fixed",
                                      transmittance="product" if storage == "f32" else "log")

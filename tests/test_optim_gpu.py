@@ -68,3 +68,35 @@ def test_bf16_gradient_adam_matches_fp32(n):
         outs.append((p, m, v, copy))
     for a, b in zip(*outs):
         assert torch.equal(a, b)
+
+
+def test_sdf_cells_adam_and_bf16_form():
+    """QSDVR_ADAM_SDF_CELLS: the same fp32 update as the element-wise step, and the bf16 copy in
+    the compensated cell form, bit-identical with qsdvr_sdf_cells_bf16 on the updated masters
+    and with the oracle's float32 restatement; the kernels read a6 as slot 6 + slot 7."""
+    import numpy as np
+
+    import oracle.oracle as O
+    from qsdvr_b200 import fused, scenes
+    from qsdvr_b200.optim import adam_step
+
+    R = 24
+    grid8 = fused.pad_grid7(scenes.procedural_grid(R, seed=3).reshape(-1, 7)).to(DEV)
+    enc = fused.sdf_cells_bf16(grid8)
+    want = O.sdf_cells_bf16(grid8.cpu().numpy())
+    assert np.array_equal(enc.cpu().view(torch.int16).numpy().view(np.uint16), want)
+    gen = torch.Generator(device=DEV).manual_seed(4)
+    g = torch.randn(grid8.shape, generator=gen, device=DEV) * 1e-3
+    g[::5] = 0.0  # whole cells without gradient keep their copy under skip_zero_grad
+    outs = []
+    for cells in (False, True):
+        p, m, v = grid8.clone(), torch.zeros_like(grid8), torch.zeros_like(grid8)
+        copy = torch.zeros(grid8.shape, dtype=torch.bfloat16, device=DEV)
+        adam_step(p, g.clone(), m, v, 1, 1e-2, param_bf16=copy, sdf_cells=cells, skip_zero_grad=True)
+        outs.append((p, m, v, copy))
+    (p0, m0, v0, c0), (p1, m1, v1, c1) = outs
+    assert torch.equal(p0, p1) and torch.equal(m0, m1) and torch.equal(v0, v1)
+    touched = g.abs().sum(1) != 0
+    assert torch.equal(c1[touched], fused.sdf_cells_bf16(p1)[touched])
+    assert torch.count_nonzero(c1[~touched]) == 0  # untouched cells were not rewritten
+    assert torch.equal(c0[touched], p0[touched].to(torch.bfloat16))

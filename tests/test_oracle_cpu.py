@@ -197,3 +197,31 @@ def test_raycut_counts_contiguous_and_offsets():
     rc = np.where(sc > 1, sc - 1, 0)
     np.testing.assert_array_equal(rays[mask, 3], np.cumsum(rc[mask]) - rc[mask])
     assert S == sc.sum() and M == rc.sum()
+
+
+def test_bf16_cell_form_keeps_the_centre_sdf():
+    """The bf16 cell form (oracle restatement of qsdvr_sdf_cells_bf16): a0..a5 are torch's
+    round-to-nearest bf16, and the decoded cell's SDF at its centre, a6 / |a3..a5| / R, equals
+    the fp32 master's to the 16 bits of the hi + lo pair, where a plain rounding misses it by
+    up to 2^-8 relative."""
+    import oracle.oracle as O
+    from qsdvr_b200 import scenes
+
+    g7 = scenes.procedural_grid(16, seed=2).reshape(-1, 7)
+    g8 = np.zeros((g7.shape[0], 8), np.float32)
+    g8[:, :7] = g7.numpy()
+    bits = O.sdf_cells_bf16(g8)
+    plain = torch.from_numpy(g8[:, :6]).to(torch.bfloat16).view(torch.int16).numpy().view(np.uint16)
+    assert np.array_equal(bits[:, :6], plain)
+    dec = O.sdf_cells_decode(bits).double().numpy()
+    m = g8.astype(np.float64)
+    centre = m[:, 6] / np.linalg.norm(m[:, 3:6], axis=1)
+    got = dec[:, 6] / np.linalg.norm(dec[:, 3:6], axis=1)
+    rel = np.abs(got - centre) / np.abs(centre)
+    assert rel.max() < 2.0 ** -16
+    pl = torch.from_numpy(g8).to(torch.bfloat16).double().numpy()
+    rel_plain = np.abs(pl[:, 6] / np.linalg.norm(pl[:, 3:6], axis=1) - centre) / np.abs(centre)
+    assert rel_plain.max() > 2.0 ** -10
+    # a plain-rounded copy (slot 7 = 0) decodes to a6 = bf16(a6)
+    pb = torch.from_numpy(g8).to(torch.bfloat16).view(torch.int16).numpy().view(np.uint16)
+    assert np.array_equal(O.sdf_cells_decode(pb).numpy()[:, 6], pl[:, 6].astype(np.float32))

@@ -5,8 +5,10 @@ plugin nothing but input and output buffers, so they cannot supply the workspace
 qsdvr_ray_cut needs.  The no-allocation variant keeps its scan scratch in a fixed array
 inside the library.  This test calls it through the C ABI twice in a row, on two different
 cameras, and checks every output against the workspace entry point (counts, offsets and
-directions are integer / bit-exact work, so the comparison is exact).  It also checks the
-size limit is enforced.  It lives in a file of its own that pytest collects last.
+directions are integer / bit-exact work, so the comparison is exact), at exactly the size
+limit (2048 x 2048, every slot of the fixed array in use) against the same entry point, and
+with no pixels (totals zero).  It also checks the size limit is enforced.  It lives in a file
+of its own that pytest collects last.
 """
 import ctypes
 
@@ -83,3 +85,28 @@ def test_ray_cut_noalloc_rejects_oversized_pixel_count():
                                    _p(dummy), None)
     assert st == 1
     assert "exceeds the fixed scratch limit" in lib.qsdvr_last_error().decode()
+
+
+def test_ray_cut_noalloc_at_the_limit_and_empty():
+    from qsdvr_b200 import scenes
+
+    L, lib = _lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    w = h = 2048
+    P = w * h
+    assert P == 4194304  # QSDVR_RAY_CUT_NOALLOC_MAX_PIXELS: all scan blocks of the fixed array
+    cam = scenes.look_at((1.1, -3.6, 1.3), w, h, 1.2 * w, 2.0, 6.0).to_c()
+    mask = (torch.rand(P, generator=torch.Generator().manual_seed(5)) < 0.7).to(torch.uint8).to(DEV)
+    want = _with_workspace(L, cam, mask, P, 4.0 / 128, stream)
+    got = _no_alloc(L, lib, cam, mask, P, 4.0 / 128, stream)
+    torch.cuda.synchronize()
+    for a, b in zip(got, want):
+        assert torch.equal(a, b)
+    assert int(got[3][0]) > 0
+    rays, origin, direction, totals = _buffers(4)
+    totals.fill_(7)
+    st = lib.qsdvr_ray_cut_noalloc(ctypes.byref(cam), _p(mask), _p(rays), _p(origin), _p(direction), 4.0 / 128, 0,
+                                   _p(totals), stream)
+    assert st == 0, lib.qsdvr_last_error().decode()
+    torch.cuda.synchronize()
+    assert totals.tolist() == [0, 0]
