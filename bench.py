@@ -330,7 +330,8 @@ def run_ours(args, cfg, device, ws, rank):
         if ev is not None:
             ev[0].record(stream)
         fused.render_train(b["target"], b["rays"], b["origin"], b["dir"], sdf_k, data_k, R, cfg["interval"],
-                           K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color, order=order)
+                           K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color, order=order,
+                           merge=args.merge)
         if ev is not None:
             ev[1].record(stream)
 
@@ -374,7 +375,7 @@ def run_ours(args, cfg, device, ws, rank):
         order = fused.ray_order(buf["rays"], buf["origin"], buf["dir"], cfg["interval"])
         fused.render_train(buf["target"], buf["rays"], buf["origin"], buf["dir"], sdf_k, data_k, R,
                            cfg["interval"], K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color,
-                           order=order)
+                           order=order, merge=args.merge)
         if ev is not None:
             ev[1].record(stream)
         released[i % 2].record(stream)
@@ -411,8 +412,9 @@ def run_ours(args, cfg, device, ws, rank):
         "config": {"workload": f"{args.workload}: R={R}^3 quadric + ({R + 1})^3x{32 if cfg.get('sh', 2) == 2 else 64} "
                                f"appearance grid, {storage}, "
                                f"{cfg['rays']} random rays/step from {cfg['views']} views at {cfg['size']}^2, "
-                               f"interval {cfg['interval']:.6g} (256 samples/ray), SH degree {cfg.get('sh', 2)}, "
-                               f"{mode} mode, k={K_LOGISTIC}",
+                               f"interval {cfg['interval']:.6g} ({round(4.0 / cfg['interval'])} samples/ray), SH degree {cfg.get('sh', 2)}, "
+                               f"{mode} mode, k={K_LOGISTIC}"
+                               + (", same-cell merged appearance scatter" if args.merge else ""),
                    "global_batch": cfg["rays"] * ws, "samples_per_step": round(mean_samples),
                    "step": "ray-order keys + sort (rays taken in Morton order of their midpoints), then one "
                            "fused forward/MSE/backward launch; gradients accumulated into buffers zeroed "
@@ -477,7 +479,8 @@ def full_step_parts(args, cfg, batches, sdf, data, sdf_k, data_k, sg, dg, mode, 
         loss.zero_()
         order = fused.ray_order(b["rays"], b["origin"], b["dir"], cfg["interval"])
         fused.render_train(b["target"], b["rays"], b["origin"], b["dir"], sdf_k, data_k, cfg["R"], cfg["interval"],
-                           K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color, order=order)
+                           K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color, order=order,
+                           merge=args.merge)
         adam()
 
     full_ms = timed(full, max(3, args.steps // 2))
@@ -806,6 +809,8 @@ def main():
     ap.add_argument("--workload", default="plain256", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-rays", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--merge", action="store_true",
+                    help="same-cell merged appearance scatter (samples of a chunk in one cell send one RED per row)")
     ap.add_argument("--no-proposal", action="store_true", help="skip the proposal-path comparison")
     ap.add_argument("--proposal-warmup", type=float, default=0.2,
                     help="fraction of the proposal run's steps trained with the uniform march first")

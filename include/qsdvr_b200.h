@@ -276,6 +276,11 @@ typedef struct qsdvr_render_args {
                                   accumulated as bf16 (each contribution and each sum rounded to
                                   8 significant bits, half the gradient traffic); no reference
                                   counterpart.  The SDF gradient stays fp32.                     */
+    int32_t merge_scatter;     /* nonzero: the render samples of a warp chunk (32 consecutive
+                                  samples of a ray) that lie in the same cell are found with one
+                                  match_any, and their appearance gradients go out as one summed
+                                  RED per corner row instead of one per sample (same sums up to
+                                  float reassociation); 0: one RED per sample and corner row   */
 } qsdvr_render_args;
 
 /* Sort keys that make neighbouring rays in a batch cross neighbouring cells (no counterpart

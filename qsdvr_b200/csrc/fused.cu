@@ -55,6 +55,11 @@ struct Rows {
     static constexpr int kPerStep = kWarp / kLanes;
 };
 constexpr uint32_t kMaxChunks = 64;  // render samples per ray <= 2048
+// Each staged tile row carries 4 floats of padding (the row stride keeps the row-wise and
+// lane-wise float4 accesses bank-conflict free); the gather and the scatter keep there the
+// sample's (base vertex, wx, wy, wz), the vertex kNoVertex for a sample without a row, so a
+// step reads one sample's parameters with one 16-byte shared load instead of 5 shuffles.
+constexpr uint32_t kNoVertex = 0xffffffffu;
 
 enum Pass { kForward = 0, kBackward = 1, kTrain = 2 };
 
@@ -113,6 +118,7 @@ struct Params {
     uint64_t sample_capacity;
     const uint32_t *order;  // optional: the i-th ray taken is order[i]
     bool grad_bf16;         // data_grad holds bf16 values
+    bool merge;             // samples of a chunk in the same cell send one summed RED per corner row
 };
 
 constexpr uint32_t kListT = 33;  // list sampling: 33 SDF positions, 32 render samples per ray
@@ -440,6 +446,12 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     s.vbase = kCompat ? (uint32_t)s.cr.index
                       : (uint32_t)s.cr.cx + (uint32_t)s.cr.cy * R1 + (uint32_t)s.cr.cz * (R1 * R1);
     const int q = lane % kL;
+    const uint32_t sy = R1, sz = R1 * R1;
+    [[maybe_unused]] const uint64_t nv = (uint64_t)R1 * R1 * R1;  // vertex rows
+    if (!from_slot) {
+        st4(tile + lane * kRow + kC, make_float4(__uint_as_float(s.shaded ? s.vbase : kNoVertex), s.wx, s.wy, s.wz));
+        __syncwarp();
+    }
     if (from_slot) {
         // rows stashed by the forward, one row per kL lanes per warp instruction
         const uint64_t pol = evict_last_policy();
@@ -448,18 +460,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
             const int j = st * kPS + lane / kL;
             st4(tile + j * kRow + 4 * q, ld4_keep(from_slot + j * kC + 4 * q, pol));
         }
-        __syncwarp();
-        if (s.shaded) {
-            s.rgb = shade_any<kCompat, kDeg>(s.nrm, d, tile + lane * kRow, &s.spec);
-        } else {
-            s.rgb = f3{0.0f, 0.0f, 0.0f};
-            s.spec = f3{0.0f, 0.0f, 0.0f};
-        }
-        return;
-    }
-    const uint32_t sy = R1, sz = R1 * R1;
-    [[maybe_unused]] const uint64_t nv = (uint64_t)R1 * R1 * R1;  // vertex rows
-    if constexpr (sizeof(S) == 2) {
+    } else if constexpr (sizeof(S) == 2) {
         // bf16 storage: groups of kGL lanes fetch one sample's 8 corner rows as 16-byte
         // (bf16 x 8) loads, kGPS samples per step; each lane stages 8 interpolated channels
         using GL = GatherLanes<S, kDeg>;
@@ -468,10 +469,10 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
 #pragma unroll kGatherUnroll
         for (int st = 0; st < kGL; ++st) {
             const int j = st * kGPS + lane / kGL;
-            const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
-            const float gx = __shfl_sync(kFull, s.wx, j), gy = __shfl_sync(kFull, s.wy, j),
-                        gz = __shfl_sync(kFull, s.wz, j);
-            const bool gok = __shfl_sync(kFull, s.shaded, j);
+            const float4 prm = ld4(tile + j * kRow + kC);
+            const uint32_t vb = __float_as_uint(prm.x);
+            const float gx = prm.y, gy = prm.z, gz = prm.w;
+            const bool gok = vb != kNoVertex;
             float v[8];
             if (gok) {
                 const uint4 v000 = Store<S>::oct(p.data, vb, q8, kC, nv), v001 = Store<S>::oct(p.data, vb + 1, q8, kC, nv);
@@ -512,10 +513,10 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
 #pragma unroll kGatherUnroll
     for (int st = 0; st < kL; ++st) {
         const int j = st * kPS + lane / kL;
-        const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
-        const float gx = __shfl_sync(kFull, s.wx, j), gy = __shfl_sync(kFull, s.wy, j),
-                    gz = __shfl_sync(kFull, s.wz, j);
-        const bool gok = __shfl_sync(kFull, s.shaded, j);
+        const float4 prm = ld4(tile + j * kRow + kC);
+        const uint32_t vb = __float_as_uint(prm.x);
+        const float gx = prm.y, gy = prm.z, gz = prm.w;
+        const bool gok = vb != kNoVertex;
         float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (gok) {
             const float4 v000 = Store<S>::quad(p.data, vb, q, kC, nv), v001 = Store<S>::quad(p.data, vb + 1, q, kC, nv);
@@ -540,6 +541,8 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
         if (to_slot) st4_keep(to_slot + j * kC + 4 * q, v, evict_last_policy());
     }
     }
+    // one shading call site for both the gathered and the stashed rows (the kernel's code
+    // size sets how often its warps wait for instruction fetch)
     __syncwarp();
     if (s.shaded) {
         // the row stays in shared memory; the shader reads the channels it needs from it
@@ -645,40 +648,68 @@ __device__ __forceinline__ void red4_bf16(__nv_bfloat16 *p, float4 v) {
     asm volatile("red.global.add.noftz.v2.bf16x2 [%0], {%1, %2};" ::"l"(p), "r"(lo), "r"(hi) : "memory");
 }
 
+// The 8 corner contributions of one sample's gradient quad g at trilinear weights (px, py,
+// pz), corner t = 4z + 2y + x (kernel/render.cu:136-151).
+__device__ __forceinline__ void corner_grads(float4 g, float px, float py, float pz, float4 *v) {
+    const float dx = 1 - px, dy = 1 - py;
+    const float4 a0 = scale4(g, 1 - pz), a1 = scale4(g, pz);
+    const float4 a00 = scale4(a0, dy), a01 = scale4(a0, py), a10 = scale4(a1, dy), a11 = scale4(a1, py);
+    v[0] = scale4(a00, dx); v[1] = scale4(a00, px); v[2] = scale4(a01, dx); v[3] = scale4(a01, px);
+    v[4] = scale4(a10, dx); v[5] = scale4(a10, px); v[6] = scale4(a11, dx); v[7] = scale4(a11, px);
+}
+__device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+
 // Scatter the data-gradient tile (rows of 32 channels per lane's sample) through the
 // trilinear weights: 8 lanes per sample, one 16-byte RED (8 bytes for a bf16 gradient) per
-// lane and corner.
+// lane and corner.  With p.merge, samples of the chunk that lie in the same cell (same base
+// vertex) are found with one match_any: the first of them sums the others' weighted
+// contributions (their gradient rows and weights read from the tile) and sends one RED per
+// corner row for all of them; the others send nothing.
 template <int kDeg>
-__device__ __forceinline__ void scatter_tile(const Params &p, const float *tile, const Sample &s, int lane) {
+__device__ __forceinline__ void scatter_tile(const Params &p, float *tile, const Sample &s, int lane) {
     using RW = Rows<kDeg>;
     constexpr int kC = RW::kC, kRow = RW::kStride, kL = RW::kLanes, kPS = RW::kPerStep;
     const uint32_t R1 = p.R + 1, sy = R1, sz = R1 * R1;
     [[maybe_unused]] const uint64_t ne = (uint64_t)kC * R1 * R1 * R1;  // gradient elements
     const int q = lane % kL;
+    uint32_t others = 0;  // p.merge: the later samples of this lane's cell, summed into this one
+    bool follower = false;
+    if (p.merge) {
+        const uint32_t key = s.valid ? s.vbase : (0x80000000u | (uint32_t)lane);  // vertices < 2^31
+        const uint32_t peers = __match_any_sync(kFull, key);
+        follower = (peers & ((1u << lane) - 1u)) != 0;  // a lower lane of the same cell leads
+        others = follower ? 0u : (peers & ~(1u << lane));
+    }
+    // the row pad: (base vertex, or kNoVertex for a sample that sends nothing, and weights)
+    st4(tile + lane * kRow + kC,
+        make_float4(__uint_as_float(s.valid && !follower ? s.vbase : kNoVertex), s.wx, s.wy, s.wz));
+    __syncwarp();
 #pragma unroll 2
     for (int st = 0; st < kL; ++st) {
         const int j = st * kPS + lane / kL;
-        const uint32_t vb = __shfl_sync(kFull, s.vbase, j);
-        const float px = __shfl_sync(kFull, s.wx, j), py = __shfl_sync(kFull, s.wy, j),
-                    pz = __shfl_sync(kFull, s.wz, j);
-        const bool ok = __shfl_sync(kFull, s.valid, j);
-        if (!ok) continue;
-        const float4 g = ld4(tile + j * kRow + 4 * q);
+        const uint32_t more = p.merge ? __shfl_sync(kFull, others, j) : 0u;
+        const float4 w = ld4(tile + j * kRow + kC);
+        const uint32_t vb = __float_as_uint(w.x);
+        if (vb == kNoVertex) continue;
         // A sample with alpha = 0 (the SDF does not fall across its interval) or T = 0 has a
         // zero appearance gradient, as do channels its shader never reads: its 8 REDs would
         // add zeros, yet each costs an L2 read-modify-write of a row that is usually not
         // cached.  Skipped; the sums stay bit-identical (is_zero4).
-        if (is_zero4(g)) continue;
-        // kernel/render.cu:136-151
-        const float dx = 1 - px, dy = 1 - py;
-        const float4 a0 = scale4(g, 1 - pz), a1 = scale4(g, pz);
-        const float4 a00 = scale4(a0, dy), a01 = scale4(a0, py), a10 = scale4(a1, dy), a11 = scale4(a1, py);
+        const float4 g = ld4(tile + j * kRow + 4 * q);
+        if (is_zero4(g) && more == 0u) continue;
+        float4 v[8];
+        corner_grads(g, w.y, w.z, w.w, v);  // kernel/render.cu:136-151
+        for (uint32_t m = more; m; m &= m - 1) {  // rare: the other samples of the same cell
+            const int f = __ffs(m) - 1;
+            const float4 gf = ld4(tile + f * kRow + 4 * q), wf = ld4(tile + f * kRow + kC);
+            const float wx[2] = {1 - wf.y, wf.y}, wy[2] = {1 - wf.z, wf.z}, wz[2] = {1 - wf.w, wf.w};
+#pragma unroll
+            for (int t = 0; t < 8; ++t) v[t] = add4(v[t], scale4(gf, wz[t >> 2] * wy[(t >> 1) & 1] * wx[t & 1]));
+        }
         const uint64_t o = (uint64_t)kC * vb + 4 * q;
         const uint64_t c[8] = {o, o + kC, o + (uint64_t)kC * sy, o + (uint64_t)kC * sy + kC, o + (uint64_t)kC * sz,
                                o + (uint64_t)kC * sz + kC, o + (uint64_t)kC * (sz + sy),
                                o + (uint64_t)kC * (sz + sy) + kC};
-        const float4 v[8] = {scale4(a00, dx), scale4(a00, px), scale4(a01, dx), scale4(a01, px),
-                             scale4(a10, dx), scale4(a10, px), scale4(a11, dx), scale4(a11, px)};
         if (p.grad_bf16) {
             __nv_bfloat16 *b = reinterpret_cast<__nv_bfloat16 *>(p.data_grad);
 #pragma unroll
@@ -690,6 +721,120 @@ __device__ __forceinline__ void scatter_tile(const Params &p, const float *tile,
     }
 }
 
+
+// Backward of one chunk given its per-sample state (eval_chunk) and transmittance T: the
+// compositing backward (compat: the reference's Tac / (alpha - 1) form; fixed: the
+// division-free reverse affine scan), dalpha/dsdf, the quadric-cell gradients and the
+// appearance scatter.  suf and next_this carry the suffix state to the preceding chunk.
+template <bool kCompat, typename S, int kDeg>
+__device__ __forceinline__ void backward_chunk(const Params &p, f3 o, f3 d, uint32_t nr, uint32_t c, int lane,
+                                               float *tile, const Sample &s, float T, f3 g, f3 &suf,
+                                               float &next_this) {
+    constexpr int kRow = Rows<kDeg>::kStride;
+    const float a = s.alpha;
+    const uint32_t i = c * kWarp + lane;
+    float dl = 0.0f;  // dL/dalpha_i
+    if (kCompat) {
+        // kernel/render.cu:279-313: Tac = sum over later samples of T a c
+        f3 v = s.valid ? f3{s.rgb.x * T * a, s.rgb.y * T * a, s.rgb.z * T * a} : f3{0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int off = 1; off < kWarp; off <<= 1) {
+            const float x = __shfl_down_sync(kFull, v.x, off), y = __shfl_down_sync(kFull, v.y, off),
+                        z = __shfl_down_sync(kFull, v.z, off);
+            if (lane + off < kWarp) {
+                v.x += x;
+                v.y += y;
+                v.z += z;
+            }
+        }
+        f3 after{__shfl_down_sync(kFull, v.x, 1), __shfl_down_sync(kFull, v.y, 1),
+                 __shfl_down_sync(kFull, v.z, 1)};
+        if (lane == kWarp - 1) after = f3{0.0f, 0.0f, 0.0f};
+        after.x += suf.x;
+        after.y += suf.y;
+        after.z += suf.z;
+        if (s.valid) {
+            const f3 dc{s.rgb.x * T + after.x / (a - 1), s.rgb.y * T + after.y / (a - 1),
+                        s.rgb.z * T + after.z / (a - 1)};
+            dl = g.x * dc.x + g.y * dc.y + g.z * dc.z;
+        }
+        suf.x += __shfl_sync(kFull, v.x, 0);
+        suf.y += __shfl_sync(kFull, v.y, 0);
+        suf.z += __shfl_sync(kFull, v.z, 0);
+    } else {
+        // R_i = a_i c_i + (1 - a_i) R_{i+1}: reverse scan of affine maps, no division
+        f3 A = s.valid ? f3{a * s.rgb.x, a * s.rgb.y, a * s.rgb.z} : f3{0.0f, 0.0f, 0.0f};
+        float B = s.valid ? 1.0f - a : 1.0f;
+#pragma unroll
+        for (int off = 1; off < kWarp; off <<= 1) {
+            const float x = __shfl_down_sync(kFull, A.x, off), y = __shfl_down_sync(kFull, A.y, off),
+                        z = __shfl_down_sync(kFull, A.z, off), b = __shfl_down_sync(kFull, B, off);
+            if (lane + off < kWarp) {
+                A.x += B * x;
+                A.y += B * y;
+                A.z += B * z;
+                B *= b;
+            }
+        }
+        const f3 Ri{A.x + B * suf.x, A.y + B * suf.y, A.z + B * suf.z};
+        f3 Rn{__shfl_down_sync(kFull, Ri.x, 1), __shfl_down_sync(kFull, Ri.y, 1),
+              __shfl_down_sync(kFull, Ri.z, 1)};
+        if (lane == kWarp - 1) Rn = suf;
+        if (s.valid) dl = T * (g.x * (s.rgb.x - Rn.x) + g.y * (s.rgb.y - Rn.y) + g.z * (s.rgb.z - Rn.z));
+        suf = f3{__shfl_sync(kFull, Ri.x, 0), __shfl_sync(kFull, Ri.y, 0), __shfl_sync(kFull, Ri.z, 0)};
+    }
+    // dalpha/dsdf (kernel/render.cu:271-278), zero where alpha == 0
+    float d_this = 0.0f, d_next = 0.0f;
+    if (s.valid && a != 0.0f) interval_dalpha<kCompat>(s.e0, s.e1, p.k, &d_next, &d_this);
+    const float mine_this = dl * d_this;
+    float from_next = __shfl_down_sync(kFull, mine_this, 1);
+    if (lane == kWarp - 1) from_next = next_this;
+    next_this = __shfl_sync(kFull, mine_this, 0);
+    if (s.valid) {
+        // SDF sample i+1 and, for the ray's first lane, SDF sample 0
+        const float gs1 = dl * d_next + (i + 1 < nr ? from_next : 0.0f);
+        float a1[7], gq[7];
+        load_cell<S>(p, s.c1, a1);
+        quad_sdf_grad(a1, s.c1.u, (float)p.R, gs1, gq);
+        // rgb gradient; 0 for an unshaded sample (alpha = 0) unless the ray's colour
+        // gradient is not finite (a NaN colour), which the reference spreads to
+        // every sample of the ray: then the unshaded one takes the full path too
+        // (its zero row gives the same NaN outputs as the real row would)
+        const f3 grgb{g.x * T * a, g.y * T * a, g.z * T * a};
+        if (s.shaded || !(isfinite(grgb.x) && isfinite(grgb.y) && isfinite(grgb.z))) {
+            // rgb gradient -> shader backward (data gradient into the tile, normal gradient)
+            // data gradient written over the data row (every read precedes its write)
+            const f3 gn =
+                shade_any_backward_inplace<kCompat, kDeg>(grgb, s.nrm, d, tile + lane * kRow, s.spec);
+            float ar[7], gr[6];
+            load_cell<S>(p, s.cr, ar);
+            sample_normal_grad<kCompat>(ar, s.cr.u, gn, gr);
+            if (s.cr.index == s.c1.index) {
+#pragma unroll
+                for (int t = 0; t < 6; ++t) gq[t] += gr[t];
+                scatter_cell(p, s.c1, gq);
+            } else {
+                scatter_cell(p, s.c1, gq);
+                const float g7[7] = {gr[0], gr[1], gr[2], gr[3], gr[4], gr[5], 0.0f};
+                scatter_cell(p, s.cr, g7);
+            }
+        } else {
+            // alpha = 0: the colour's gradients (data row, normal) are 0 and the row
+            // in the tile is the gather's zeros, which the scatter skips
+            scatter_cell(p, s.c1, gq);
+        }
+        if (i == 0) {
+            const CellPoint c0 = to_cell(march(o, d, 0.0f, p.interval), p.volume_offset, p.R);
+            float a0[7], g0[7];
+            load_cell<S>(p, c0, a0);
+            quad_sdf_grad(a0, c0.u, (float)p.R, mine_this, g0);
+            scatter_cell(p, c0, g0);
+        }
+    }
+    __syncwarp();
+    scatter_tile<kDeg>(p, tile, s, lane);
+    __syncwarp();
+}
 
 template <bool kCompat, typename S, int kPass, bool kLogT, int kDeg>
 __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kernel(const Params p) {
@@ -743,8 +888,8 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
         Transmittance<kLogT> tr;
         float ts_lo = 0.0f, ts_hi = 0.0f;  // transmittance carry at the start of chunk lane / lane+32
         float T_last = 0.0f;               // transmittance of this lane's sample in the last chunk
-        // ---------------- forward
-        if (kPass != kBackward || run) {
+        // ---------------- forward (forward and backward-only passes)
+        if (kPass == kForward || (kPass == kBackward && run)) {
             if (run) {
                 f3 acc{0.0f, 0.0f, 0.0f};
                 for (uint32_t c = 0; c < chunks; ++c) {
@@ -755,12 +900,8 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                         eval_alpha<kCompat, S>(p, r, o, d, nr, c, lane, s);
                         tr.step(s.alpha, s.valid, lane);
                     } else {
-                        float *stash = (slot && c + 1 < chunks && c + 1 + kSlotChunks >= chunks)
-                                           ? slot + (c % kSlotChunks) * kChunkFloats
-                                           : nullptr;
-                        eval_chunk<kCompat, S, kDeg>(p, r, o, d, nr, c, lane, tile, s, nullptr, stash);
+                        eval_chunk<kCompat, S, kDeg>(p, r, o, d, nr, c, lane, tile, s);
                         const float T = tr.step(s.alpha, s.valid, lane);
-                        T_last = T;
                         if (p.sample_alpha && c * kWarp + lane < nr) {
                             const uint64_t m = (uint64_t)info.render_offset + c * kWarp + lane;
                             if (m < p.sample_capacity) p.sample_alpha[m] = s.alpha;
@@ -774,140 +915,77 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                 }
                 C = f3{warp_sum(acc.x), warp_sum(acc.y), warp_sum(acc.z)};
             }
-            if (kPass != kBackward && lane == 0) store3(QSDVR_AT(p.color, 3ull * r, 3, 3ull * p.n), C);
+            if (kPass == kForward && lane == 0) store3(QSDVR_AT(p.color, 3ull * r, 3, 3ull * p.n), C);
         }
-        // ---------------- loss gradient
-        f3 g{0.0f, 0.0f, 0.0f};
-        if (kPass == kTrain) {
-            const f3 t = load3(QSDVR_AT(p.target, 3ull * r, 3, 3ull * p.n));
-            const f3 e{C.x - t.x, C.y - t.y, C.z - t.z};
-            if (lane == 0) sq += e.x * e.x + e.y * e.y + e.z * e.z;  // C is warp-uniform: count it once
-            g = f3{p.grad_scale * e.x, p.grad_scale * e.y, p.grad_scale * e.z};
-        } else if (kPass == kBackward) {
-            g = load3(QSDVR_AT(p.grad_color, 3ull * r, 3, 3ull * p.n));
-        }
-        // ---------------- backward (chunks in reverse, suffix state carried)
-        if (kPass != kForward && run) {
+        if (kPass == kBackward && run) {
+            const f3 g = load3(QSDVR_AT(p.grad_color, 3ull * r, 3, 3ull * p.n));
             f3 suf{0.0f, 0.0f, 0.0f};  // compat: sum_{m>chunk} T a c ; fixed: R after the chunk
             float next_this = 0.0f;    // d_this term of the first sample of the following chunk
             for (int c = (int)chunks - 1; c >= 0; --c) {
+                tr.carry = __shfl_sync(kFull, c < 32 ? ts_lo : ts_hi, c & 31);
+                eval_chunk<kCompat, S, kDeg>(p, r, o, d, nr, (uint32_t)c, lane, tile, s);
+                const float T = tr.step(s.alpha, s.valid, lane);
+                backward_chunk<kCompat, S, kDeg>(p, o, d, nr, (uint32_t)c, lane, tile, s, T, g, suf, next_this);
+            }
+        }
+        // ---------------- train: the forward chunks, the MSE gradient, then the chunks in
+        // reverse, as one loop with one chunk evaluation (one inlined copy of the gather and
+        // shading code; the kernel's code size sets how often its warps wait for instruction
+        // fetch).  The last forward chunk's rows and per-sample state stay in the tile and in
+        // registers for the first backward step; stashed rows serve the chunks before it.
+        if (kPass == kTrain) {
+            f3 g{0.0f, 0.0f, 0.0f};
+            f3 acc{0.0f, 0.0f, 0.0f};
+            f3 suf{0.0f, 0.0f, 0.0f};
+            float next_this = 0.0f;
+            const uint32_t total = run ? 2 * chunks : 0;
+            for (uint32_t it = 0;; ++it) {
+                if (it == (run ? chunks : 0)) {
+                    // end of the forward: colour, loss and its gradient
+                    C = f3{warp_sum(acc.x), warp_sum(acc.y), warp_sum(acc.z)};
+                    if (lane == 0) store3(QSDVR_AT(p.color, 3ull * r, 3, 3ull * p.n), C);
+                    const f3 t = load3(QSDVR_AT(p.target, 3ull * r, 3, 3ull * p.n));
+                    const f3 e{C.x - t.x, C.y - t.y, C.z - t.z};
+                    if (lane == 0) sq += e.x * e.x + e.y * e.y + e.z * e.z;  // C is warp-uniform: count it once
+                    g = f3{p.grad_scale * e.x, p.grad_scale * e.y, p.grad_scale * e.z};
+                }
+                if (it >= total) break;
+                const bool fwd = it < chunks;
+                const uint32_t c = fwd ? it : total - 1 - it;  // backward: chunks - 1 down to 0
                 float T;
-                if (kPass == kTrain && c == (int)chunks - 1) {
+                if (fwd || c + 1 < chunks) {
+                    if (fwd) {
+                        if ((c & 31) == (uint32_t)lane) {
+                            if (c < 32) ts_lo = tr.carry; else ts_hi = tr.carry;
+                        }
+                    } else {
+                        tr.carry = __shfl_sync(kFull, c < 32 ? ts_lo : ts_hi, c & 31);
+                    }
+                    float *sl = (slot && c + 1 < chunks && c + 1 + kSlotChunks >= chunks)
+                                    ? slot + (c % kSlotChunks) * kChunkFloats
+                                    : nullptr;
+                    eval_chunk<kCompat, S, kDeg>(p, r, o, d, nr, c, lane, tile, s, fwd ? nullptr : sl,
+                                                 fwd ? sl : nullptr);
+                    T = tr.step(s.alpha, s.valid, lane);
+                } else {
                     // the forward just evaluated this chunk: its rows are still in the tile and
                     // its per-sample state in registers, so nothing is fetched again
                     T = T_last;
+                }
+                if (fwd) {
+                    T_last = T;
+                    if (p.sample_alpha && c * kWarp + lane < nr) {
+                        const uint64_t m = (uint64_t)info.render_offset + c * kWarp + lane;
+                        if (m < p.sample_capacity) p.sample_alpha[m] = s.alpha;
+                        else flag_error(QSDVR_DEVERR_CAPACITY);
+                    }
+                    acc.x += s.rgb.x * s.alpha * T;
+                    acc.y += s.rgb.y * s.alpha * T;
+                    acc.z += s.rgb.z * s.alpha * T;
+                    __syncwarp();
                 } else {
-                    const float t0 = __shfl_sync(kFull, c < 32 ? ts_lo : ts_hi, c & 31);
-                    tr.carry = t0;
-                    const float *stashed = (slot && (uint32_t)c + 1 + kSlotChunks >= chunks)
-                                               ? slot + ((uint32_t)c % kSlotChunks) * kChunkFloats
-                                               : nullptr;
-                    eval_chunk<kCompat, S, kDeg>(p, r, o, d, nr, (uint32_t)c, lane, tile, s, stashed);
-                    T = tr.step(s.alpha, s.valid, lane);
+                    backward_chunk<kCompat, S, kDeg>(p, o, d, nr, c, lane, tile, s, T, g, suf, next_this);
                 }
-                const float a = s.alpha;
-                const uint32_t i = (uint32_t)c * kWarp + lane;
-                float dl = 0.0f;  // dL/dalpha_i
-                if (kCompat) {
-                    // kernel/render.cu:279-313: Tac = sum over later samples of T a c
-                    f3 v = s.valid ? f3{s.rgb.x * T * a, s.rgb.y * T * a, s.rgb.z * T * a} : f3{0.0f, 0.0f, 0.0f};
-#pragma unroll
-                    for (int off = 1; off < kWarp; off <<= 1) {
-                        const float x = __shfl_down_sync(kFull, v.x, off), y = __shfl_down_sync(kFull, v.y, off),
-                                    z = __shfl_down_sync(kFull, v.z, off);
-                        if (lane + off < kWarp) {
-                            v.x += x;
-                            v.y += y;
-                            v.z += z;
-                        }
-                    }
-                    f3 after{__shfl_down_sync(kFull, v.x, 1), __shfl_down_sync(kFull, v.y, 1),
-                             __shfl_down_sync(kFull, v.z, 1)};
-                    if (lane == kWarp - 1) after = f3{0.0f, 0.0f, 0.0f};
-                    after.x += suf.x;
-                    after.y += suf.y;
-                    after.z += suf.z;
-                    if (s.valid) {
-                        const f3 dc{s.rgb.x * T + after.x / (a - 1), s.rgb.y * T + after.y / (a - 1),
-                                    s.rgb.z * T + after.z / (a - 1)};
-                        dl = g.x * dc.x + g.y * dc.y + g.z * dc.z;
-                    }
-                    suf.x += __shfl_sync(kFull, v.x, 0);
-                    suf.y += __shfl_sync(kFull, v.y, 0);
-                    suf.z += __shfl_sync(kFull, v.z, 0);
-                } else {
-                    // R_i = a_i c_i + (1 - a_i) R_{i+1}: reverse scan of affine maps, no division
-                    f3 A = s.valid ? f3{a * s.rgb.x, a * s.rgb.y, a * s.rgb.z} : f3{0.0f, 0.0f, 0.0f};
-                    float B = s.valid ? 1.0f - a : 1.0f;
-#pragma unroll
-                    for (int off = 1; off < kWarp; off <<= 1) {
-                        const float x = __shfl_down_sync(kFull, A.x, off), y = __shfl_down_sync(kFull, A.y, off),
-                                    z = __shfl_down_sync(kFull, A.z, off), b = __shfl_down_sync(kFull, B, off);
-                        if (lane + off < kWarp) {
-                            A.x += B * x;
-                            A.y += B * y;
-                            A.z += B * z;
-                            B *= b;
-                        }
-                    }
-                    const f3 Ri{A.x + B * suf.x, A.y + B * suf.y, A.z + B * suf.z};
-                    f3 Rn{__shfl_down_sync(kFull, Ri.x, 1), __shfl_down_sync(kFull, Ri.y, 1),
-                          __shfl_down_sync(kFull, Ri.z, 1)};
-                    if (lane == kWarp - 1) Rn = suf;
-                    if (s.valid) dl = T * (g.x * (s.rgb.x - Rn.x) + g.y * (s.rgb.y - Rn.y) + g.z * (s.rgb.z - Rn.z));
-                    suf = f3{__shfl_sync(kFull, Ri.x, 0), __shfl_sync(kFull, Ri.y, 0), __shfl_sync(kFull, Ri.z, 0)};
-                }
-                // dalpha/dsdf (kernel/render.cu:271-278), zero where alpha == 0
-                float d_this = 0.0f, d_next = 0.0f;
-                if (s.valid && a != 0.0f) interval_dalpha<kCompat>(s.e0, s.e1, p.k, &d_next, &d_this);
-                const float mine_this = dl * d_this;
-                float from_next = __shfl_down_sync(kFull, mine_this, 1);
-                if (lane == kWarp - 1) from_next = next_this;
-                next_this = __shfl_sync(kFull, mine_this, 0);
-                if (s.valid) {
-                    // SDF sample i+1 and, for the ray's first lane, SDF sample 0
-                    const float gs1 = dl * d_next + (i + 1 < nr ? from_next : 0.0f);
-                    float a1[7], gq[7];
-                    load_cell<S>(p, s.c1, a1);
-                    quad_sdf_grad(a1, s.c1.u, (float)p.R, gs1, gq);
-                    // rgb gradient; 0 for an unshaded sample (alpha = 0) unless the ray's colour
-                    // gradient is not finite (a NaN colour), which the reference spreads to
-                    // every sample of the ray: then the unshaded one takes the full path too
-                    // (its zero row gives the same NaN outputs as the real row would)
-                    const f3 grgb{g.x * T * a, g.y * T * a, g.z * T * a};
-                    if (s.shaded || !(isfinite(grgb.x) && isfinite(grgb.y) && isfinite(grgb.z))) {
-                        // rgb gradient -> shader backward (data gradient into the tile, normal gradient)
-                        // data gradient written over the data row (every read precedes its write)
-                        const f3 gn =
-                            shade_any_backward_inplace<kCompat, kDeg>(grgb, s.nrm, d, tile + lane * kRow, s.spec);
-                        float ar[7], gr[6];
-                        load_cell<S>(p, s.cr, ar);
-                        sample_normal_grad<kCompat>(ar, s.cr.u, gn, gr);
-                        if (s.cr.index == s.c1.index) {
-#pragma unroll
-                            for (int t = 0; t < 6; ++t) gq[t] += gr[t];
-                            scatter_cell(p, s.c1, gq);
-                        } else {
-                            scatter_cell(p, s.c1, gq);
-                            const float g7[7] = {gr[0], gr[1], gr[2], gr[3], gr[4], gr[5], 0.0f};
-                            scatter_cell(p, s.cr, g7);
-                        }
-                    } else {
-                        // alpha = 0: the colour's gradients (data row, normal) are 0 and the row
-                        // in the tile is the gather's zeros, which the scatter skips
-                        scatter_cell(p, s.c1, gq);
-                    }
-                    if (i == 0) {
-                        const CellPoint c0 = to_cell(march(o, d, 0.0f, p.interval), p.volume_offset, p.R);
-                        float a0[7], g0[7];
-                        load_cell<S>(p, c0, a0);
-                        quad_sdf_grad(a0, c0.u, (float)p.R, mine_this, g0);
-                        scatter_cell(p, c0, g0);
-                    }
-                }
-                __syncwarp();
-                scatter_tile<kDeg>(p, tile, s, lane);
-                __syncwarp();
             }
         }
     }
@@ -1029,6 +1107,7 @@ int launch(const qsdvr_render_args *a, cudaStream_t stream) {
     p.sample_capacity = a->sample_capacity;
     p.order = a->order;
     p.grad_bf16 = a->data_grad_storage == QSDVR_STORAGE_BF16;
+    p.merge = a->merge_scatter != 0;
     unsigned blocks = grid_for(a->ray_count, kWarpsPerBlock);
     if (a->workspace) {
         const Layout L = layout_for(a, kPass);

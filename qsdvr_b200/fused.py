@@ -33,7 +33,8 @@ class RenderArgs(ctypes.Structure):
                 ("sdf_grid", P), ("data", P), ("color", P), ("target", P), ("grad_color", P), ("sdf_grad", P),
                 ("data_grad", P), ("loss", P), ("grad_scale", F32), ("workspace", P), ("workspace_bytes", ctypes.c_uint64),
                 ("sdf_layers", P), ("sdf_layers_grad", P), ("tlist", P), ("sample_alpha", P),
-                ("sample_capacity", ctypes.c_uint64), ("order", P), ("data_grad_storage", I32)]
+                ("sample_capacity", ctypes.c_uint64), ("order", P), ("data_grad_storage", I32),
+                ("merge_scatter", I32)]
 
 
 _lib.extra_signatures({
@@ -101,7 +102,7 @@ def _grid_storage(sdf_grid, data, R):
 def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat", transmittance="product",
               color=None, target=None, grad_color=None, sdf_grad=None, data_grad=None, loss=None,
               grad_scale=0.0, persistent=True, tlist=None, sample_alpha=None, sdf_layers=None,
-              sdf_layers_grad=None, order=None) -> RenderArgs:
+              sdf_layers_grad=None, order=None, merge=False) -> RenderArgs:
     dev, n = _check_batch(rays, origin, direction)
     a = RenderArgs()
     a.rays, a.origin, a.dir = _ptr(rays), _ptr(origin), _ptr(direction)
@@ -127,6 +128,7 @@ def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="
     a.color, a.target, a.grad_color = _ptr(color), _ptr(target), _ptr(grad_color)
     a.sdf_grad, a.data_grad, a.loss = _ptr(sdf_grad), _ptr(data_grad), _ptr(loss)
     a.grad_scale = float(grad_scale)
+    a.merge_scatter = 1 if merge else 0
     a.workspace, a.workspace_bytes = None, 0
     if tlist is not None:
         if tlist.device != dev or tlist.dtype != torch.float32 or tlist.shape != (n, 33) or not tlist.is_contiguous():
@@ -189,7 +191,7 @@ def render_forward(rays, origin, direction, sdf_grid, data, reso, interval, k, m
 
 def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
                     mode="compat", transmittance="product", persistent=True, tlist=None, sdf_layers=None,
-                    order=None):
+                    order=None, merge=False):
     """Accumulate dL/d(sdf_grid) (fp32) and dL/d(data) (fp32, or bf16 when ``data_grad`` is a
     bfloat16 tensor) for a given dL/dcolor.  With ``sdf_layers``, ``sdf_grad`` is the tables'
     gradient ([3R+1,4], see ``separable_grad``)."""
@@ -202,19 +204,20 @@ def render_backward(grad_color, rays, origin, direction, sdf_grid, data, reso, i
     a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode, transmittance, grad_color=g,
                   sdf_grad=None if sdf_layers is not None else sdf_grad, data_grad=data_grad,
                   persistent=persistent, tlist=tlist, sdf_layers=sdf_layers,
-                  sdf_layers_grad=sdf_grad if sdf_layers is not None else None, order=order)
+                  sdf_layers_grad=sdf_grad if sdf_layers is not None else None, order=order, merge=merge)
     with torch.cuda.device(dev):
         call("qsdvr_render_backward", ctypes.byref(a), _stream(dev))
 
 
 def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval, k, sdf_grad, data_grad,
                  mode="compat", transmittance="product", loss=None, color=None, persistent=True, tlist=None,
-                 sample_alpha=None, sdf_layers=None, order=None):
+                 sample_alpha=None, sdf_layers=None, order=None, merge=False):
     """Forward + MSE (mean over N x 3) + backward in one launch.  Returns (color, loss_sum)
     where loss_sum accumulates sum |color - target|^2 (divide by 3N for the mean).  With
     ``sdf_layers``, ``sdf_grad`` is the tables' gradient ([3R+1,4]).  A bfloat16 ``data_grad``
     accumulates the appearance gradient in bf16 (half its traffic; the SDF gradient stays
-    fp32)."""
+    fp32).  ``merge``: samples of a warp chunk in the same cell send one summed appearance
+    RED per corner row (the kernel's same-cell merge)."""
     dev, n = _check_batch(rays, origin, direction)
     if color is None:
         color = torch.empty((n, 3), dtype=torch.float32, device=dev)
@@ -225,7 +228,7 @@ def render_train(target, rays, origin, direction, sdf_grid, data, reso, interval
                   target=target.contiguous(), sdf_grad=None if sep else sdf_grad, data_grad=data_grad, loss=loss,
                   grad_scale=2.0 / (3.0 * max(n, 1)), persistent=persistent, tlist=tlist,
                   sample_alpha=sample_alpha, sdf_layers=sdf_layers, sdf_layers_grad=sdf_grad if sep else None,
-                  order=order)
+                  order=order, merge=merge)
     with torch.cuda.device(dev):
         call("qsdvr_render_train", ctypes.byref(a), _stream(dev))
     return color, loss
