@@ -65,27 +65,39 @@ WORKLOADS = {
     # 256^3 scene: proposal path against the uniform march, rays/s and held-out PSNR
     "train512": dict(R=256, rays=65536, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 512,
                      storage="f32"),
+    # the reference's small CPU-runnable case: a 64^3 noisy sphere, one 100x100 view at radius 4
+    # (focal 138.9), 64 samples/ray, every pixel's ray, MSE against a seeded U(0,1) image
+    "config1": dict(R=64, rays=10000, views=1, size=100, focal=138.9, radius=4.0, interval=4.0 / 64,
+                    storage="f32", scene="sphere"),
 }
+CONFIG1_CAMERA = (0.0, -4.0, 0.0)  # radius 4, looking at the origin
 PROPOSAL_STEPS = 300  # training steps per method in the default line's proposal comparison
 
 
-def byte_terms(storage: str, sh: int, grad: str = "f32") -> tuple[int, int]:
-    """Algorithmic bytes of the train kernel: (per render sample, per active sample).  Every
-    sample reads its two quadric cells and sends their gradient (192).  An active sample,
-    one with alpha > 0, also gathers its 8 corner rows once (8 C b; the backward rereads
+def byte_terms(storage: str, sh: int, grad: str = "f32") -> tuple[int, int, int]:
+    """Algorithmic bytes of the train kernel: (per render sample, per sample whose SDF sample
+    has a gradient, per active sample).  Every sample reads its two quadric cells (SDF sample
+    i+1 and the render sample's cell, 2 x 32 B).  The SDF sample's cell gradient is
+    read-modify-written (64 B) when it is not zero, i.e. when alpha > 0 on either interval the
+    sample bounds.  An active sample, one with alpha > 0, also read-modify-writes its render
+    cell's normal gradient (64 B), gathers its 8 corner rows once (8 C b; the backward rereads
     them from the warp's L2 stash) and read-modify-writes its 8 gradient rows in L2
-    (2 x 8 C g).  An inactive sample contributes nothing to the colour: its rows are
-    neither gathered nor sent.  C channels, b storage bytes, g gradient bytes."""
+    (2 x 8 C g).  An inactive sample's colour terms are all zero: its rows are neither
+    gathered nor sent.  C channels, b storage bytes, g gradient bytes."""
     c = 32 if sh == 2 else 64
     b = 4 if storage == "f32" else 2
     g = 4 if grad == "f32" else 2
-    return 192, 8 * c * b + 2 * 8 * c * g
+    return 64, 64, 64 + 8 * c * b + 2 * 8 * c * g
 
 
-def bytes_per_sample(storage: str, sh: int, grad: str = "f32", active: float = 1.0) -> float:
-    """Algorithmic bytes per render sample when a fraction ``active`` of them is active."""
-    every, per_active = byte_terms(storage, sh, grad)
-    return every + active * per_active
+def bytes_per_sample(storage: str, sh: int, grad: str = "f32", active: float = 1.0,
+                     sdf_grad: float | None = None) -> float:
+    """Algorithmic bytes per render sample when a fraction ``active`` of them is active and a
+    fraction ``sdf_grad`` (default: ``active``) sends an SDF-cell gradient."""
+    every, per_sdf, per_active = byte_terms(storage, sh, grad)
+    return every + (active if sdf_grad is None else sdf_grad) * per_sdf + active * per_active
+
+
 BYTES_PER_RAY = 64  # origin + dir in, target in, colour out, RayInfo
 K_LOGISTIC = 5.0
 METRIC = "train rays/s fwd+bwd @256^3 grid (256 samples/ray, 65536-ray batches)"
@@ -212,6 +224,13 @@ def build_scene(cfg, device, seed):
     from qsdvr_b200.camera import Camera
 
     R = cfg["R"]
+    if cfg.get("scene") == "sphere":  # config1: the model is the noisy sphere; targets are U(0,1)
+        cam = Camera(scenes.look_at(CONFIG1_CAMERA, cfg["size"], cfg["size"], cfg["focal"], 2.0, 6.0),
+                     cfg["interval"], R, device=device)
+        cam.GenerateRayPoints(torch.ones(cfg["size"] * cfg["size"], dtype=torch.bool))
+        sdf = fused.pad_grid7(scenes.sphere_grid(R, 0.5, 0.01, seed=seed, device=device).reshape(-1, 7))
+        data = scenes.appearance(R, seed=seed, device=device)
+        return dict(gt=None, model=(sdf, data), rays=cam.rayList, origin=cam.originList, dir=cam.dirList)
     gt_sdf = fused.pad_grid7(scenes.procedural_grid(R, seed=seed, device=device).reshape(-1, 7))
     sh = cfg.get("sh", 2)
     gt_data = scenes.appearance(R, seed=seed, device=device, procedural=True, sh_degree=sh)
@@ -234,6 +253,9 @@ def build_scene(cfg, device, seed):
 def make_batches(scene, cfg, count, device, seed):
     from qsdvr_b200 import fused
 
+    if scene["gt"] is None:  # config1: every pixel's ray in pixel order, targets U(0,1) (seed 0)
+        target = torch.rand((scene["rays"].shape[0], 3), generator=torch.Generator().manual_seed(0)).to(device)
+        return [dict(rays=scene["rays"], origin=scene["origin"], dir=scene["dir"], target=target)] * count
     gen = torch.Generator(device=device).manual_seed(seed)
     total = scene["rays"].shape[0]
     out = []
@@ -254,19 +276,26 @@ def samples_of(batch):
 
 
 def active_samples_of(batch, sdf_k, data_k, R, interval, mode, transmittance):
-    """Render samples of the batch with alpha > 0 under the model (outside any timed region):
-    one forward of the library with its per-sample alpha output, the ray records given packed
-    render offsets (the fused kernels read only sdf_count besides)."""
+    """(samples with alpha > 0, samples whose SDF sample has a gradient: alpha > 0 on its own
+    interval or on the next one of the same ray) under the model, counted outside any timed
+    region with one forward of the library and its per-sample alpha output (the ray records
+    given packed render offsets; the fused kernels read only sdf_count besides)."""
     from qsdvr_b200 import fused
 
     rays = batch["rays"].clone()
     cnt = torch.clamp(rays[:, 0].long() - 1, min=0)
     rays[:, 2] = cnt.to(torch.int32)
-    rays[:, 3] = (torch.cumsum(cnt, 0) - cnt).to(torch.int32)
+    off = torch.cumsum(cnt, 0) - cnt
+    rays[:, 3] = off.to(torch.int32)
     alpha = torch.zeros(int(cnt.sum()), dtype=torch.float32, device=rays.device)
     fused.render_forward(rays, batch["origin"], batch["dir"], sdf_k, data_k, R, interval, K_LOGISTIC, mode,
                          transmittance, sample_alpha=alpha)
-    return int((alpha > 0).sum())
+    act = alpha > 0
+    nxt = torch.zeros_like(act)
+    nxt[:-1] = act[1:]
+    last = (off + cnt - 1)[cnt > 0]  # a ray's last sample has no next interval in the ray
+    nxt[last] = False
+    return int(act.sum()), int((act | nxt).sum())
 
 
 # ----------------------------------------------------------------------------- timing
@@ -344,8 +373,10 @@ def run_ours(args, cfg, device, ws, rank):
         torch.distributed.barrier()
     # samples with a non-zero appearance gradient under the model the timed region used (the
     # full-step timing below updates the model)
-    active = [active_samples_of(b, sdf_k, data_k, R, cfg["interval"], mode, transmittance) for b in batches]
-    active_frac = sum(active) / max(1, sum(samples_of(b) for b in batches))
+    counts = [active_samples_of(b, sdf_k, data_k, R, cfg["interval"], mode, transmittance) for b in batches]
+    all_samples = max(1, sum(samples_of(b) for b in batches))
+    active_frac = sum(c[0] for c in counts) / all_samples
+    sdf_grad_frac = sum(c[1] for c in counts) / all_samples
     # ---- e2e through the public API with host buffers (pinned), copies inside the region
     host = []
     for b in batches:
@@ -395,13 +426,14 @@ def run_ours(args, cfg, device, ws, rank):
     # ---- roofline of the train kernel
     samples = [samples_of(b) for b in batches]
     mean_samples = sum(samples) / len(samples)
-    bps = bytes_per_sample(storage, cfg.get("sh", 2), cfg.get("grad", "f32"), active_frac)
+    bps = bytes_per_sample(storage, cfg.get("sh", 2), cfg.get("grad", "f32"), active_frac, sdf_grad_frac)
     alg_bytes = mean_samples * bps + cfg["rays"] * BYTES_PER_RAY
     achieved = alg_bytes / (kern_avg / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
     tps = profiled_traffic_per_sample(storage + ("_sh3" if cfg.get("sh", 2) == 3 else "")
                                       + ("_grad_bf16" if cfg.get("grad", "f32") == "bf16" else ""))
-    traffic = None if tps is None else tps * mean_samples
+    # the committed DRAM capture covers the 256^3 workloads only
+    traffic = None if tps is None or R != 256 else tps * mean_samples
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "rays/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
@@ -411,8 +443,9 @@ def run_ours(args, cfg, device, ws, rank):
         "data": "synthetic (seeded procedural scene, random-init sphere model)",
         "config": {"workload": f"{args.workload}: R={R}^3 quadric + ({R + 1})^3x{32 if cfg.get('sh', 2) == 2 else 64} "
                                f"appearance grid, {storage}, "
-                               f"{cfg['rays']} random rays/step from {cfg['views']} views at {cfg['size']}^2, "
-                               f"interval {cfg['interval']:.6g} ({round(4.0 / cfg['interval'])} samples/ray), SH degree {cfg.get('sh', 2)}, "
+                               + (f"every pixel's ray of one {cfg['size']}^2 view, " if cfg.get("scene") == "sphere"
+                                  else f"{cfg['rays']} random rays/step from {cfg['views']} views at {cfg['size']}^2, ")
+                               + f"interval {cfg['interval']:.6g} ({round(4.0 / cfg['interval'])} samples/ray), SH degree {cfg.get('sh', 2)}, "
                                f"{mode} mode, k={K_LOGISTIC}"
                                + (", same-cell merged appearance scatter" if args.merge else ""),
                    "global_batch": cfg["rays"] * ws, "samples_per_step": round(mean_samples),
@@ -429,10 +462,12 @@ def run_ours(args, cfg, device, ws, rank):
                      "kernel": "render_kernel<train>", "kernel_ms": round(kern_avg, 4),
                      "algorithmic_bytes": round(alg_bytes), "bytes_per_sample": round(bps, 1),
                      "active_sample_fraction": round(active_frac, 4),
+                     "sdf_grad_sample_fraction": round(sdf_grad_frac, 4),
                      "peak_kind": peak_kind},
         "clocks": clk.summary(),
     }
-    if ws == 1 and not args.no_cpu_baseline and cfg.get("sh", 2) == 2:  # the reference's CPU path is SH degree 2
+    # the reference's CPU path is SH degree 2; config1's full case is timed by --impl reference
+    if ws == 1 and not args.no_cpu_baseline and cfg.get("sh", 2) == 2 and cfg.get("scene") != "sphere":
         out["cpu_baseline"] = cpu_baseline(scene, batches[0], cfg, args.cpu_rays)
     if ws == 1 and args.workload == "plain256" and not args.no_proposal:
         del scene, batches
@@ -761,41 +796,90 @@ def cpu_baseline(scene, batch, cfg, n_rays, steps=1):
                       f"{os.cpu_count()}"}
 
 
+def reference_batch_cpu(cfg, n_rays, seed=0):
+    """A bounded sample of the workload built on the host alone, with the oracle: the model
+    grids of the GPU arm (same seeds), ``n_rays`` pixels drawn at random over the same seeded
+    views and marched by the oracle's RayCut (oracle/raygen.c), and their targets rendered by
+    the oracle (float32, fixed mode) from the ground-truth scene.  config1 takes every pixel of
+    its one view and a seeded U(0,1) target image.  Nothing here loads the product library."""
+    import oracle.oracle as O
+    from qsdvr_b200 import scenes
+
+    R = cfg["R"]
+    if cfg.get("scene") == "sphere":
+        a = scenes.look_at(CONFIG1_CAMERA, cfg["size"], cfg["size"], cfg["focal"], 2.0, 6.0)
+        cam = O.Camera(a.width, a.height, tuple(a.rotation), tuple(a.translation), a.fx, a.fy, a.cx, a.cy, a.near,
+                       a.far)
+        rays, origin, direction, _, _ = O.ray_cut(cam, np.ones(a.width * a.height, np.uint8), cfg["interval"])
+        grid7 = scenes.sphere_grid(R, 0.5, 0.01, seed=seed).reshape(-1, 7).contiguous()
+        data = scenes.appearance(R, seed=seed)
+        target = torch.rand((rays.shape[0], 3), generator=torch.Generator().manual_seed(0))
+        return grid7, data, dict(rays=rays, rays_packed=rays, origin=origin, dir=direction, target=target)
+    cams = scenes.hemisphere_cameras(cfg["views"], cfg["radius"], cfg["size"], cfg["size"], cfg["focal"], 2.0, 6.0,
+                                     seed=seed)
+    rng = np.random.default_rng(1000 + seed)
+    views = rng.integers(0, len(cams), n_rays)
+    pixels = rng.integers(0, cfg["size"] * cfg["size"], n_rays)
+    rays = np.zeros((n_rays, 4), np.uint32)
+    origin = np.zeros((n_rays, 3), np.float32)
+    direction = np.zeros((n_rays, 3), np.float32)
+    for i, (v, px) in enumerate(zip(views, pixels)):
+        a = cams[v]
+        cam = O.Camera(a.width, a.height, tuple(a.rotation), tuple(a.translation), a.fx, a.fy, a.cx, a.cy, a.near,
+                       a.far)
+        r, o, d = O.ray_cut_pixels(cam, np.array([px], np.uint32), cfg["interval"])
+        rays[i], origin[i], direction[i] = r[0], o[0], d[0]
+    c = rays[:, 0].astype(np.int64)
+    rc = np.maximum(c - 1, 0)
+    rays[:, 1] = np.cumsum(c) - c
+    rays[:, 2] = rc
+    rays[:, 3] = np.cumsum(rc) - rc
+    pts = O.generate_ray_points(rays, origin, direction, cfg["interval"], R)
+    inp = {k: torch.from_numpy(v) for k, v in pts.items()}
+    inp["rayList"] = torch.from_numpy(rays.astype(np.int64))
+    gt7 = scenes.procedural_grid(R, seed=seed).reshape(-1, 7)
+    gt_data = scenes.appearance(R, seed=seed, procedural=True)
+    with torch.no_grad():
+        target = O.render(gt7, gt_data, inp, K_LOGISTIC, compat=False).float()
+    del gt7, gt_data
+    grid7 = scenes.sphere_grid(R, 0.5, 0.01, seed=seed).reshape(-1, 7).contiguous()
+    data = scenes.appearance(R, seed=seed + 1)
+    return grid7, data, dict(rays=rays, rays_packed=rays, origin=origin, dir=direction, target=target)
+
+
 def run_reference(args, cfg):
-    """The reference's CPU implementation timed on the host cores (rank 0 only)."""
+    """The reference's CPU implementation timed on the host cores (rank 0 only); its batch is
+    built on the host by the oracle (reference_batch_cpu)."""
     if cfg.get("sh", 2) != 2:
         print(json.dumps({"impl": "reference", "unavailable": "the reference renders SH degree 2 only"}))
         return
     torch.set_num_threads(os.cpu_count() or 1)
-    device = torch.device("cuda", 0) if torch.cuda.is_available() else None
-    if device is None:
-        print(json.dumps({"impl": "reference", "unavailable": "no CUDA device to build the synthetic scene"}))
-        return
-    scene = build_scene(cfg, device, seed=0)
-    batch = make_batches(scene, cfg, 1, device, seed=1000)[0]
-    sdf, data = scene["model"]
-    grid7 = sdf[:, :7].contiguous().cpu()
-    data_cpu = data.cpu()
-    del scene
-    b = _cpu_batch(batch, args.cpu_rays)
+    n = cfg["rays"] if cfg.get("scene") == "sphere" else args.cpu_rays
+    grid7, data_cpu, b = reference_batch_cpu(cfg, n)
+    n = b["rays"].shape[0]
     for _ in range(args.warmup):
         _cpu_step(grid7, data_cpu, b, cfg["R"], cfg["interval"])
     t0 = time.perf_counter()
     for _ in range(args.steps):
         _cpu_step(grid7, data_cpu, b, cfg["R"], cfg["interval"])
     dt = time.perf_counter() - t0
-    value = args.cpu_rays * args.steps / dt
+    value = n * args.steps / dt
+    samples = int(np.maximum(b["rays"][:, 0].astype(np.int64) - 1, 0).sum())
+    full = cfg.get("scene") == "sphere"
+    sample = (f"all {n} rays of the view ({samples} render samples)" if full else
+              f"{n} rays per step drawn at random over the {cfg['views']} views ({samples} render samples) of the "
+              f"{cfg['rays']}-ray batch's ray pool")
     # n_gpus mirrors the launch (--gpus N); the timed work runs on rank 0's host cores
     line = {"metric": METRIC, "impl": "reference", "value": round(value, 2), "unit": "rays/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (same seeded scene and batch as the GPU arm)",
-            "config": {"workload": f"{args.workload}: bounded sample of {args.cpu_rays} rays per step of the "
-                                   f"{cfg['rays']}-ray batch", "global_batch": args.cpu_rays},
+            "data": "synthetic (the GPU arm's seeded scene; rays and targets made on the host by the oracle)",
+            "config": {"workload": f"{args.workload}: " + ("full case" if full else "bounded sample") + f", {sample}",
+                       "global_batch": n},
             "cpu_baseline": {"value": round(value, 2), "unit": "rays/s", "cores": torch.get_num_threads(),
                              "kind": "port",
-                             "sample": f"{args.cpu_rays} rays/step, reference torch render path (per-ray loop) "
-                                       f"fwd+bwd on the host"},
+                             "sample": f"{sample}; reference torch render path (models/render_torch.py, per-ray "
+                                       f"loop) fwd+bwd on the host; os.cpu_count()={os.cpu_count()}"},
             "e2e": {"value": round(value, 2), "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 

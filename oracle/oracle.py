@@ -85,6 +85,7 @@ def _lib():
         lib.oracle_generate_ray_points.argtypes = [P, P, P, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32,
                                                    P, P, P, P, P]
         lib.oracle_list_points.argtypes = [P, P, P, ctypes.c_uint32, P, ctypes.c_uint32, P, P, P, P, P]
+        lib.oracle_ray_cut_pixels.argtypes = [ctypes.POINTER(_Camera), P, ctypes.c_uint32, ctypes.c_float, P, P, P]
         _raygen = lib
     return _raygen
 
@@ -135,6 +136,20 @@ def ray_cut(cam: Camera, mask: np.ndarray, interval: float, rays_prev: np.ndarra
     _lib().oracle_ray_cut(ctypes.byref(c), _ptr(mask), P, ctypes.c_float(interval), _ptr(rays), _ptr(origin),
                           _ptr(direction), _ptr(totals))
     return rays, origin, direction, int(totals[0]), int(totals[1])
+
+
+def ray_cut_pixels(cam: Camera, pixels: np.ndarray, interval: float):
+    """kernel/camera.cu:12-58 for a list of pixel ids: (rays [n,4] uint32 with packed offsets
+    in list order, counts < 2 zeroed; origin [n,3]; dir [n,3])."""
+    pixels = np.ascontiguousarray(pixels, np.uint32)
+    n = pixels.size
+    rays = np.zeros((n, 4), np.uint32)
+    origin = np.zeros((n, 3), np.float32)
+    direction = np.zeros((n, 3), np.float32)
+    c = cam._c()
+    _lib().oracle_ray_cut_pixels(ctypes.byref(c), _ptr(pixels), n, ctypes.c_float(interval), _ptr(rays), _ptr(origin),
+                                 _ptr(direction))
+    return rays, origin, direction
 
 
 def generate_ray_points(rays: np.ndarray, origin: np.ndarray, direction: np.ndarray, interval: float, reso: int):

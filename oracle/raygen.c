@@ -110,6 +110,26 @@ void oracle_ray_cut(const oracle_camera *cam, const uint8_t *mask, uint32_t pixe
     totals[1] = render_total;
 }
 
+/* The records of a list of pixels (each marched as camera.cu:12-58 does), with packed
+ * exclusive-scan offsets in list order: the host-side ray batch of the benchmark's CPU arm
+ * (a random sample of pixels over many views) without marching every pixel of a view. */
+void oracle_ray_cut_pixels(const oracle_camera *cam, const uint32_t *pixels, uint32_t count, float interval,
+                           uint32_t *rays, float *origin, float *dir)
+{
+    uint32_t sdf_total = 0, render_total = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        uint32_t cnt = ray_cut_pixel(cam, pixels[i], interval, dir + 3 * i, origin + 3 * i);
+        if (cnt < 2) cnt = 0;
+        uint32_t *r = rays + 4 * i;
+        r[0] = cnt;
+        r[1] = sdf_total;
+        sdf_total += cnt;
+        r[2] = cnt > 1 ? cnt - 1 : 0;
+        r[3] = render_total;
+        render_total += r[2];
+    }
+}
+
 /* camera.cu:73-80 / 86-93: world point to (local coords in [-1,1), cell index). */
 static void to_cell(const float p_in[3], float volume_offset, uint32_t reso, float local[3], int32_t *index)
 {
