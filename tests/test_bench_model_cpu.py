@@ -34,7 +34,6 @@ def test_reference_arm_batch_is_built_on_the_host():
     import numpy as np
 
     import bench
-    from qsdvr_b200 import _lib
 
     cfg = dict(bench.WORKLOADS["plain128"], R=16, views=3, size=40, focal=55.0)
     grid7, data, b = bench.reference_batch_cpu(cfg, 12)
@@ -46,4 +45,12 @@ def test_reference_arm_batch_is_built_on_the_host():
     full = dict(bench.WORKLOADS["config1"], R=16)
     _, _, fb = bench.reference_batch_cpu(full, 0)
     assert fb["rays"].shape == (100 * 100, 4) and int((fb["rays"][:, 0] >= 2).sum()) > 1000
-    assert _lib._lib is None  # nothing above loaded libqsdvr_b200.so
+    # a fresh process that builds such a batch never maps the product library
+    import subprocess
+    import sys
+
+    code = ("import bench; cfg = dict(bench.WORKLOADS['plain128'], R=16, views=2, size=24, focal=33.0); "
+            "bench.reference_batch_cpu(cfg, 4); print('libqsdvr_b200' in open('/proc/self/maps').read())")
+    out = subprocess.run([sys.executable, "-c", code], cwd=bench.ROOT, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert out.stdout.strip().splitlines()[-1] == "False"
