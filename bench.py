@@ -496,32 +496,53 @@ def full_step_parts(args, cfg, batches, sdf, data, sdf_k, data_k, sg, dg, mode, 
         return a.elapsed_time(b) / reps
 
     zero_ms = timed(lambda: (sg.zero_(), dg.zero_()), 5)
+    # the share of parameters one step's gradient touches (non-zero after one train launch)
+    sg.zero_(), dg.zero_()
+    b0 = batches[0]
+    order0 = fused.ray_order(b0["rays"], b0["origin"], b0["dir"], cfg["interval"])
+    fused.render_train(b0["target"], b0["rays"], b0["origin"], b0["dir"], sdf_k, data_k, cfg["R"], cfg["interval"],
+                       K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color, order=order0)
+    touched_rows = float((dg.reshape(dg.shape[0], -1) != 0).any(1).float().mean())
+    touched = float(((sg != 0).sum() + (dg != 0).sum()) / (sg.numel() + dg.numel()))
     params = [sdf.clone(), data.clone()]
     grads = [sg, dg]
     moments = [(torch.zeros_like(q), torch.zeros_like(q)) for q in params]
+    moments16 = [(torch.zeros_like(q, dtype=torch.bfloat16), torch.zeros_like(q, dtype=torch.bfloat16))
+                 for q in params]
     copies = [sdf_k, data_k] if sdf_k.dtype == torch.bfloat16 else [None, None]
     count = [0]
 
-    def adam():
+    def adam(state=moments, lazy=False, zero=True):
         count[0] += 1
-        for j, (q, g, (m, v), c) in enumerate(zip(params, grads, moments, copies)):
-            adam_step(q, g, m, v, count[0], 1e-3, param_bf16=c, sdf_cells=(j == 0))
+        for j, (q, g, (m, v), c) in enumerate(zip(params, grads, state, copies)):
+            adam_step(q, g, m, v, count[0], 1e-3, param_bf16=c, sdf_cells=(j == 0), skip_zero_grad=lazy,
+                      zero_grad=zero)
 
     adam_ms = timed(adam, 5)
+    adam16_ms = timed(lambda: adam(moments16), 5)
+    # the lazy step on one real gradient (not zeroed in between, so each repetition sees it)
+    fused.render_train(b0["target"], b0["rays"], b0["origin"], b0["dir"], sdf_k, data_k, cfg["R"], cfg["interval"],
+                       K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color, order=order0)
+    lazy_ms = timed(lambda: adam(lazy=True, zero=False), 5)
+    sg.zero_(), dg.zero_()
 
-    def full():
+    def full(state=moments):
         b = batches[count[0] % len(batches)]
         loss.zero_()
         order = fused.ray_order(b["rays"], b["origin"], b["dir"], cfg["interval"])
         fused.render_train(b["target"], b["rays"], b["origin"], b["dir"], sdf_k, data_k, cfg["R"], cfg["interval"],
                            K_LOGISTIC, sg, dg, mode, transmittance, loss=loss, color=color, order=order,
                            merge=args.merge)
-        adam()
+        adam(state)
 
     full_ms = timed(full, max(3, args.steps // 2))
-    del params, moments
+    full16_ms = timed(lambda: full(moments16), max(3, args.steps // 2))
+    del params, moments, moments16
     return {"zero_grad_ms": round(zero_ms, 4), "adam_ms": round(adam_ms, 4),
+            "adam_bf16_state_ms": round(adam16_ms, 4), "adam_lazy_ms": round(lazy_ms, 4),
+            "touched_param_fraction": round(touched, 4), "touched_vertex_row_fraction": round(touched_rows, 4),
             "full_step_ms": round(full_ms, 4), "full_step_rays_per_s": round(cfg["rays"] / (full_ms / 1e3), 1),
+            "full_step_bf16_state_ms": round(full16_ms, 4),
             "full_step": "fused forward/MSE/backward + fused Adam over both grids (fp32 masters; bf16 copies "
                          "refreshed for bf16 storage; gradients zeroed in the same pass)"}
 

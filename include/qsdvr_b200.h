@@ -326,8 +326,12 @@ enum {
     QSDVR_ADAM_ZERO_GRAD = 1,      /* write zeros over the gradient after using it           */
     QSDVR_ADAM_SKIP_ZERO_GRAD = 2, /* leave elements whose gradient is exactly 0 untouched    */
     QSDVR_ADAM_GRAD_BF16 = 4,      /* grad points to bf16 values (render data_grad_storage)  */
-    QSDVR_ADAM_SDF_CELLS = 8       /* param is a quadric cell grid [count/8][8] (fp32 grad): the
+    QSDVR_ADAM_SDF_CELLS = 8,      /* param is a quadric cell grid [count/8][8] (fp32 grad): the
                                       bf16 copy is written in the cell form of qsdvr_sdf_cells_bf16 */
+    QSDVR_ADAM_STATE_BF16 = 16     /* exp_avg and exp_avg_sq hold bf16 values (no reference
+                                      counterpart; torch keeps fp32 moments): updated in fp32 and
+                                      stochastically rounded back, 24 instead of 32 bytes of HBM
+                                      traffic per parameter */
 };
 
 /* One Adam step over `count` fp32 elements.  The default (flags without SKIP_ZERO_GRAD)
@@ -337,8 +341,8 @@ enum {
 typedef struct qsdvr_adam_args {
     float *param;
     float *grad;        /* fp32, or bf16 with QSDVR_ADAM_GRAD_BF16 */
-    float *exp_avg;
-    float *exp_avg_sq;
+    float *exp_avg;     /* fp32, or bf16 with QSDVR_ADAM_STATE_BF16 */
+    float *exp_avg_sq;  /* fp32, or bf16 with QSDVR_ADAM_STATE_BF16 */
     void *param_bf16;   /* optional [count] bf16 */
     uint64_t count;
     double lr, beta1, beta2, eps; /* host precision; the kernel's float constants are derived from them */

@@ -32,7 +32,35 @@ struct AdamParams {
     uint64_t n;
     float b1, b2, one_minus_b1, one_minus_b2, step_size, bc2_sqrt, eps;
     bool zero_grad, skip_zero;
+    bool state_bf16;  // m and v hold bf16 values, stochastically rounded after each update
+    uint32_t seed;    // per-step seed of the stochastic rounding
 };
+
+// Stochastic rounding of the bf16 moments (QSDVR_ADAM_STATE_BF16).  Adam's second moment
+// decays by beta2 = 0.999 per step, a relative change below half a bf16 ulp (2^-9), so round
+// to nearest would leave it frozen; rounding up with probability equal to the discarded
+// fraction keeps every moment unbiased.  The random bits come from a counter-based integer
+// hash (the "lowbias32" xorshift-multiply mixer) of the element group and the step.
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+__device__ __forceinline__ uint32_t sr_bf16(float x, uint32_t r16) {
+    uint32_t u = __float_as_uint(x);
+    if ((u & 0x7f800000u) != 0x7f800000u) u += r16 & 0xffffu;  // inf and NaN keep their bits
+    return u >> 16;
+}
+__device__ __forceinline__ float4 bf16x4(uint2 r) {
+    return make_float4(__uint_as_float(r.x << 16), __uint_as_float(r.x & 0xffff0000u), __uint_as_float(r.y << 16),
+                       __uint_as_float(r.y & 0xffff0000u));
+}
+__device__ __forceinline__ uint2 sr_bf16x4(float4 v, uint32_t ra, uint32_t rb) {
+    return make_uint2(sr_bf16(v.x, ra) | (sr_bf16(v.y, ra >> 16) << 16), sr_bf16(v.z, rb) | (sr_bf16(v.w, rb >> 16) << 16));
+}
 
 __device__ __forceinline__ uint32_t bf16_bits(float x) { return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x)); }
 __device__ __forceinline__ float bf16_value(uint32_t b) { return __uint_as_float(b << 16); }
@@ -97,14 +125,28 @@ __device__ __forceinline__ bool adam_group(const AdamParams &a, uint64_t i, floa
         return false;
     }
     p = ld4(a.param + 4 * i);
-    float4 m = ld4(a.m + 4 * i), v = ld4(a.v + 4 * i);
+    float4 m, v;
+    if (a.state_bf16) {
+        m = bf16x4(reinterpret_cast<const uint2 *>(a.m)[i]);
+        v = bf16x4(reinterpret_cast<const uint2 *>(a.v)[i]);
+    } else {
+        m = ld4(a.m + 4 * i);
+        v = ld4(a.v + 4 * i);
+    }
     if (!a.skip_zero || g.x != 0.0f) adam_one(p.x, g.x, m.x, v.x, a);
     if (!a.skip_zero || g.y != 0.0f) adam_one(p.y, g.y, m.y, v.y, a);
     if (!a.skip_zero || g.z != 0.0f) adam_one(p.z, g.z, m.z, v.z, a);
     if (!a.skip_zero || g.w != 0.0f) adam_one(p.w, g.w, m.w, v.w, a);
     st4(a.param + 4 * i, p);
-    st4(a.m + 4 * i, m);
-    st4(a.v + 4 * i, v);
+    if (a.state_bf16) {
+        const uint32_t h0 = mix32((uint32_t)i ^ mix32((uint32_t)(i >> 32) ^ a.seed)), h1 = mix32(h0), h2 = mix32(h1),
+                       h3 = mix32(h2);
+        reinterpret_cast<uint2 *>(a.m)[i] = sr_bf16x4(m, h0, h1);
+        reinterpret_cast<uint2 *>(a.v)[i] = sr_bf16x4(v, h2, h3);
+    } else {
+        st4(a.m + 4 * i, m);
+        st4(a.v + 4 * i, v);
+    }
     if (a.zero_grad) zero_grad4<kBf16Grad>(a, i);
     return true;
 }
@@ -126,11 +168,19 @@ __global__ void __launch_bounds__(256) adam_kernel(const AdamParams a) {
     for (uint64_t i = 4 * n4 + blockIdx.x * 256ull + threadIdx.x; i < a.n; i += stride) {
         const float g = grad1<kBf16Grad>(a, i);
         if (a.skip_zero && g == 0.0f) continue;
-        float p = a.param[i], m = a.m[i], v = a.v[i];
+        __nv_bfloat16 *mb = reinterpret_cast<__nv_bfloat16 *>(a.m), *vb = reinterpret_cast<__nv_bfloat16 *>(a.v);
+        float p = a.param[i];
+        float m = a.state_bf16 ? __bfloat162float(mb[i]) : a.m[i], v = a.state_bf16 ? __bfloat162float(vb[i]) : a.v[i];
         adam_one(p, g, m, v, a);
         a.param[i] = p;
-        a.m[i] = m;
-        a.v[i] = v;
+        if (a.state_bf16) {
+            const uint32_t h = mix32(mix32((uint32_t)i ^ a.seed) ^ 0x51ed270bu);
+            mb[i] = __ushort_as_bfloat16((unsigned short)sr_bf16(m, h));
+            vb[i] = __ushort_as_bfloat16((unsigned short)sr_bf16(v, h >> 16));
+        } else {
+            a.m[i] = m;
+            a.v[i] = v;
+        }
         if (a.zero_grad) {
             if (kBf16Grad) reinterpret_cast<__nv_bfloat16 *>(a.grad)[i] = __float2bfloat16_rn(0.0f);
             else a.grad[i] = 0.0f;
@@ -156,6 +206,15 @@ __global__ void __launch_bounds__(256) adam_cells_kernel(const AdamParams a) {
 }  // namespace qsdvr
 
 using namespace qsdvr;
+
+static uint32_t mix32_host(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
 
 extern "C" int qsdvr_adam_step(const qsdvr_adam_args *args, cudaStream_t stream) {
     if (!args) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_adam_step: null args");
@@ -186,6 +245,8 @@ extern "C" int qsdvr_adam_step(const qsdvr_adam_args *args, cudaStream_t stream)
     a.eps = (float)args->eps;
     a.zero_grad = (args->flags & QSDVR_ADAM_ZERO_GRAD) != 0;
     a.skip_zero = (args->flags & QSDVR_ADAM_SKIP_ZERO_GRAD) != 0;
+    a.state_bf16 = (args->flags & QSDVR_ADAM_STATE_BF16) != 0;
+    a.seed = mix32_host(args->step);
     const uint64_t work = (args->count + 3) / 4;
     unsigned blocks = grid_for(work, 256);
     const unsigned cap = 148u * 16;  // a few waves of resident blocks, grid-stride beyond

@@ -93,6 +93,10 @@ def parser():
     ap.add_argument("--model", default="dense", choices=["dense", "separable"],
                     help="dense quadric grid, or the reference's separable layers (RenderGrid)")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--adam-state", default="f32", choices=["f32", "bf16"],
+                    help="Adam moments in bf16 (stochastic rounding; 24 instead of 32 B per parameter and step)")
+    ap.add_argument("--lazy-adam", action="store_true",
+                    help="leave parameters whose gradient is exactly 0 untouched (their moments do not decay)")
     return ap
 
 
@@ -123,7 +127,8 @@ def run(a, data=None, quiet=False, return_state=False):
         data_grad = torch.zeros(model.renderData.shape, dtype=torch.bfloat16, device=dev)
     opt = FusedGridAdam(model.parameters(), lr=a.lr, bf16_copies=copies,
                         grads={model.renderData: data_grad} if data_grad is not None else None,
-                        sdf_cells=(model.sdfGrid,))
+                        sdf_cells=(model.sdfGrid,), skip_zero_grad=getattr(a, "lazy_adam", False),
+                        state_dtype=torch.bfloat16 if getattr(a, "adam_state", "f32") == "bf16" else torch.float32)
     model.sdfGrid.grad = torch.zeros_like(model.sdfGrid)
     if data_grad is None:
         model.renderData.grad = data_grad = torch.zeros_like(model.renderData)

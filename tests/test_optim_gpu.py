@@ -100,3 +100,39 @@ def test_sdf_cells_adam_and_bf16_form():
     assert torch.equal(c1[touched], fused.sdf_cells_bf16(p1)[touched])
     assert torch.count_nonzero(c1[~touched]) == 0  # untouched cells were not rewritten
     assert torch.equal(c0[touched], p0[touched].to(torch.bfloat16))
+
+
+def test_bf16_state_adam_tracks_fp32_state():
+    """QSDVR_ADAM_STATE_BF16: the moments live in bf16, updated in fp32 and stochastically
+    rounded back.  After one step each stored moment is one of the two bf16 neighbours of the
+    fp32-state value, unbiased on average, and the farther one a quarter of the time (as
+    stochastic rounding of uniformly placed values gives); after 5 steps the parameters stay
+    within 0.1 of one step's size of the fp32-state run."""
+    from qsdvr_b200.optim import adam_step
+
+    n = (1 << 20) + 3  # with a tail of 3 elements
+    gen = torch.Generator(device=DEV).manual_seed(5)
+    p0 = torch.randn(n, generator=gen, device=DEV)
+    grads = [torch.randn(n, generator=gen, device=DEV) * (0.2 + s) for s in range(5)]
+    lr = 1e-2
+    runs = {}
+    for dt in (torch.float32, torch.bfloat16):
+        p, m, v = p0.clone(), torch.zeros(n, dtype=dt, device=DEV), torch.zeros(n, dtype=dt, device=DEV)
+        for step, g in enumerate(grads, 1):
+            adam_step(p, g.clone(), m, v, step, lr)
+            if step == 1:
+                runs[(dt, "m1")], runs[(dt, "v1")] = m.float().clone(), v.float().clone()
+        runs[dt] = p
+    for key in ("m1", "v1"):
+        exact, got = runs[(torch.float32, key)], runs[(torch.bfloat16, key)]
+        lo = exact.to(torch.bfloat16).float()
+        ulp = (torch.nextafter(exact.to(torch.bfloat16), torch.full_like(lo, float("inf")).to(torch.bfloat16)).float()
+               - lo).abs()
+        assert ((got - exact).abs() <= 2 * ulp).all(), key
+        rel = (got - exact) / ulp.clamp_min(1e-30)
+        assert abs(float(rel.mean())) < 5e-3, key  # unbiased
+        # stochastic, not nearest: a quarter of the values go to the farther neighbour
+        far = float((rel.abs() > 0.5).float().mean())
+        assert 0.2 < far < 0.3, (key, far)
+    err = float((runs[torch.bfloat16] - runs[torch.float32]).abs().max())
+    assert err < 0.1 * lr, err  # 5 steps of ~lr each, moments within 2^-8
