@@ -462,3 +462,52 @@ def test_same_cell_merged_scatter(fz, mode):
     eb = rel_err(res[(True, torch.bfloat16)][3].float().cpu(), d0.cpu())
     assert eb < 2e-2, eb
     assert _lib.device_error() == 0
+
+
+def test_nonfinite_appearance_row_of_inactive_samples(fz):
+    """A documented divergence from the reference: a non-finite appearance row that only
+    samples with alpha = 0 read.  The reference shades every sample, so NaN x 0 makes the
+    colour of each ray that reads such a row NaN; the fused kernel neither gathers nor shades
+    those samples, so their rows never reach a colour or a gradient.  Here every row that some
+    alpha = 0 sample reads and no alpha > 0 sample reads holds NaN (compat mode, the
+    reference's addressing): the kernel's colours and gradients equal those of the same model
+    with those rows zeroed, bit for bit, and are finite; the reference (run live when built)
+    gives NaN colours on the rays that read them."""
+    from oracle.build_ref import load_reference
+    from qsdvr_b200 import scenes
+    from tests.golden.make_golden import reference_render
+
+    R, k, interval = 16, 5.0, 4.0 / 64
+    cam = camera_batch((0.3, -4.0, 0.4), 40, 55.0, interval, R)
+    grid7 = scenes.sphere_grid(R, 0.5, 0.01, seed=6).reshape(-1, 7).to(DEV)
+    grid8 = fz.pad_grid7(grid7)
+    data = scenes.appearance(R, seed=6).to(DEV)
+    pts = cam.GetRayPoints()
+    alpha = torch.zeros(pts["renderIndexList"].shape[0], device=DEV)
+    fz.render_forward(cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k, "compat",
+                      sample_alpha=alpha)
+    R1 = R + 1
+    corners = torch.tensor([0, 1, R1, R1 + 1, R1 * R1, R1 * R1 + 1, R1 * R1 + R1, R1 * R1 + R1 + 1], device=DEV)
+    rows = pts["renderIndexList"].long()[:, None] + corners[None, :]  # compat: the cell index as base vertex
+    read_active = torch.zeros(R1 ** 3, dtype=torch.bool, device=DEV)
+    read_inactive = torch.zeros_like(read_active)
+    read_active[rows[alpha > 0].reshape(-1)] = True
+    read_inactive[rows[alpha == 0].reshape(-1)] = True
+    only_inactive = read_inactive & ~read_active
+    assert int(only_inactive.sum()) > 100  # the case is exercised
+    bad, zeroed = data.clone(), data.clone()
+    bad[only_inactive] = float("nan")
+    zeroed[only_inactive] = 0.0
+    target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(7)).to(DEV)
+    out = []
+    for d in (bad, zeroed):
+        sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+        img, loss = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, grid8, d, R, interval, k, sg, dg)
+        out.append((img, loss, sg, dg))
+    (i0, l0, s0, d0), (i1, l1, s1, d1) = out
+    assert torch.isfinite(i0).all() and torch.isfinite(s0).all() and torch.isfinite(d0).all()
+    assert torch.equal(i0, i1) and torch.equal(s0, s1) and torch.equal(d0, d1)
+    ref = load_reference()
+    if ref is not None:
+        want, _, _ = reference_render(ref, grid7, bad, pts, R, k, target)
+        assert (~torch.isfinite(want)).any()  # the reference's colours on those rays are NaN
