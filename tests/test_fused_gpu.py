@@ -489,6 +489,8 @@ def test_nonfinite_appearance_row_of_inactive_samples(fz):
     R1 = R + 1
     corners = torch.tensor([0, 1, R1, R1 + 1, R1 * R1, R1 * R1 + 1, R1 * R1 + R1, R1 * R1 + R1 + 1], device=DEV)
     rows = pts["renderIndexList"].long()[:, None] + corners[None, :]  # compat: the cell index as base vertex
+    rc = rows.cpu()
+    assert int(rc.min()) >= 0 and int(rc.max()) < R1 ** 3  # checked on the host before indexing with them
     read_active = torch.zeros(R1 ** 3, dtype=torch.bool, device=DEV)
     read_inactive = torch.zeros_like(read_active)
     read_active[rows[alpha > 0].reshape(-1)] = True
