@@ -30,12 +30,16 @@ DEV = "cuda"
 
 
 def _entrywise(ours, ref, floor=1e-3):
-    """Largest |ours - ref| / |ref| over entries with |ref| > floor * max |ref|, and their count."""
+    """Largest |ours - ref| / |ref| over the finite entries with |ref| > floor * max |ref|, their
+    count, the 0.999 quantile of that error, and the count of non-finite reference entries
+    (rel_err requires ours to be non-finite at exactly those)."""
     a = ours.double().reshape(-1)
     b = ref.double().reshape(-1)
-    big = b.abs() > floor * b.abs().max()
+    fin = torch.isfinite(b)
+    big = fin & (b.abs() > floor * b[fin].abs().max())
     rel = (a[big] - b[big]).abs() / b[big].abs()
-    return float(rel.max()), int(big.sum()), float(rel.quantile(0.999)) if rel.numel() < 2 ** 24 else None
+    q = float(torch.sort(rel).values[int(0.999 * (rel.numel() - 1))]) if rel.numel() else 0.0
+    return float(rel.max()) if rel.numel() else 0.0, int(big.sum()), q, int((~fin).sum())
 
 
 def test_headline_batch_entrywise_parity_with_reference():
@@ -81,8 +85,8 @@ def test_headline_batch_entrywise_parity_with_reference():
 
     e_img = float((col - img).abs().max())
     e_sdf, e_data = rel_err(sg[:, :7].cpu(), g7.cpu()), rel_err(dg.cpu(), gd.cpu())
-    w_sdf, n_sdf, q_sdf = _entrywise(sg[:, :7], g7)
-    w_data, n_data, q_data = _entrywise(dg, gd)
+    w_sdf, n_sdf, q_sdf, nf_sdf = _entrywise(sg[:, :7], g7)
+    w_data, n_data, q_data, nf_data = _entrywise(dg, gd)
 
     # bf16 storage, appearance gradient accumulated in fp32 and in bf16 (bf16g_256)
     s16, d16 = fused.sdf_cells_bf16(sdf), data.to(torch.bfloat16)
@@ -102,6 +106,7 @@ def test_headline_batch_entrywise_parity_with_reference():
         "image_max_abs": e_img, "sdf_grad_normwise": e_sdf, "data_grad_normwise": e_data,
         "sdf_grad_entrywise_max": w_sdf, "sdf_entries_checked": n_sdf, "sdf_entrywise_q999": q_sdf,
         "data_grad_entrywise_max": w_data, "data_entries_checked": n_data, "data_entrywise_q999": q_data,
+        "nonfinite_reference_entries": [nf_sdf, nf_data],
         "bf16g_data_grad_normwise_vs_fp32_accumulation": e_bf16g, "bf16g_sdf_grad_vs_fp32": e_bf16_sdf}))
     assert e_img < 1e-5
     assert e_sdf < 1e-4 and e_data < 1e-4
