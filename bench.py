@@ -473,6 +473,8 @@ def run_ours(args, cfg, device, ws, rank):
         del scene, batches
         torch.cuda.empty_cache()
         out["proposal"] = proposal_comparison(PROPOSAL_STEPS, args.proposal_warmup)
+        # the same comparison on bf16 storage (both methods; the learned proposal form's precision)
+        out["proposal_bf16"] = proposal_comparison(PROPOSAL_STEPS, args.proposal_warmup, storage="bf16")
     return out
 
 
@@ -549,7 +551,7 @@ def full_step_parts(args, cfg, batches, sdf, data, sdf_k, data_k, sg, dg, mode, 
 
 # ----------------------------------------------------------------------------- proposal path
 
-def proposal_comparison(steps: int, warmup_frac: float = 0.2, interval: float = 4.0 / 256):
+def proposal_comparison(steps: int, warmup_frac: float = 0.2, interval: float = 4.0 / 256, storage: str = "f32"):
     """Training at 256^3 from the same initial model on the same ray pool: the uniform march
     (4 / interval samples/ray, 65536 rays/step) and the proposal path (64 coarse MLP points + 32 fine
     samples/ray, network trained online every step; twice the rays per step, which costs
@@ -560,7 +562,7 @@ def proposal_comparison(steps: int, warmup_frac: float = 0.2, interval: float = 
     from qsdvr_b200 import train
 
     a = train.parser().parse_args([])
-    a.steps, a.log_every, a.interval = steps, 10 ** 9, interval
+    a.steps, a.log_every, a.interval, a.storage = steps, 10 ** 9, interval, storage
     data = train.build(a.reso, a.views, a.size, 1111.1 * a.size / 800, 4.03, a.interval, a.k, a.seed,
                        torch.device("cuda", torch.cuda.current_device()))
     plain = train.run(a, data, quiet=True)
@@ -569,7 +571,8 @@ def proposal_comparison(steps: int, warmup_frac: float = 0.2, interval: float = 
     del data
     torch.cuda.empty_cache()
     return {"method": "64 coarse MLP points + 32 fine samples per ray (tcgen05 MLP, trained online)",
-            "workload": f"R={a.reso}^3 fp32 fixed mode, {steps} training steps per method from the same sphere "
+            "workload": f"R={a.reso}^3 {'fp32' if storage == 'f32' else 'bf16 storage (fp32 masters)'} fixed "
+                        f"mode, {steps} training steps per method from the same sphere "
                         f"init, k={a.k}, Adam lr {a.lr}; plain {plain['rays_per_step']} rays/step, proposal "
                         f"{prop['rays_per_step']} rays/step with {a.proposal_warmup} uniform warm-up steps",
             "train_rays_per_s": prop["render_rays_per_s"], "plain_train_rays_per_s": plain["render_rays_per_s"],
