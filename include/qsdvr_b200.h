@@ -291,6 +291,18 @@ typedef struct qsdvr_render_args {
 int qsdvr_ray_order_keys(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
                          float interval, uint32_t *keys, cudaStream_t stream);
 
+/* Workspace bytes of qsdvr_ray_order for ray_count rays (a 2^15 + 1 bucket histogram and one
+ * bucket per ray). */
+size_t qsdvr_ray_order_workspace_size(uint32_t ray_count);
+
+/* The ray order itself, without a library sort (no counterpart in the reference): order
+ * receives a permutation of 0..ray_count-1 that lists the rays by the 15-bit Morton code of
+ * their in-box midpoint (a 32^3 lattice of the volume), rays with fewer than 2 SDF samples
+ * last; within one lattice cube the order is the order in which the device's atomics reach
+ * the rays.  Three kernels and a memset on the stream (histogram, scan, scatter). */
+int qsdvr_ray_order(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
+                    float interval, uint32_t *order, void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
 /* Separable SDF for the fused renderer (the RenderGrid model's parametrisation,
  * models/render.py:172-207, without materialising [R^3][7]; LayerToGridForward,
  * kernel/surface.cu:148-229, computes the same cells): per-axis recurrence tables

@@ -1200,6 +1200,86 @@ __global__ void __launch_bounds__(256) ray_order_keys_kernel(const qsdvr_ray_inf
     keys[r] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
 }
 
+// Ray order by counting sort: the 15-bit Morton code of each ray's in-box midpoint (5 bits
+// per axis, a 32^3 lattice of the volume; rays without samples in one extra last bucket),
+// a histogram, its exclusive scan, and a scatter that lists each bucket's rays in the order
+// the scatter reaches them.  Rays in one bucket lie within one 1/16-wide cube of the volume,
+// the locality the render kernels need; finer keys order rays within such a cube, which does
+// not change what the rays in flight share.
+constexpr uint32_t kOrderBuckets = (1u << 15) + 1;
+
+__device__ __forceinline__ uint32_t ray_bucket(const qsdvr_ray_info *rays, const float *origin, const float *dir,
+                                               uint32_t r, float interval) {
+    const uint32_t ns = rays[r].sdf_count;
+    if (ns < 2) return kOrderBuckets - 1;
+    const float t = 0.5f * (float)(ns - 1) * interval;
+    const f3 o = load3(origin + 3ull * r), d = load3(dir + 3ull * r);
+    const float c[3] = {fmaf(d.x, t, o.x), fmaf(d.y, t, o.y), fmaf(d.z, t, o.z)};
+    uint32_t q[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) q[a] = (uint32_t)fminf(fmaxf((c[a] + 1.0f) * 16.0f, 0.0f), 31.0f);
+    return spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+}
+
+__global__ void __launch_bounds__(256) ray_bucket_kernel(const qsdvr_ray_info *__restrict__ rays,
+                                                         const float *__restrict__ origin,
+                                                         const float *__restrict__ dir, uint32_t n, float interval,
+                                                         uint32_t *__restrict__ bucket, uint32_t *__restrict__ hist) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint32_t b = ray_bucket(rays, origin, dir, r, interval);
+    bucket[r] = b;
+    atomicAdd(hist + b, 1u);
+}
+
+// Exclusive scan of the kOrderBuckets counts in place, one block of 1024 threads.
+__global__ void __launch_bounds__(1024) bucket_scan_kernel(uint32_t *__restrict__ hist) {
+    constexpr uint32_t kPer = (kOrderBuckets + 1023) / 1024;
+    __shared__ uint32_t warp_sums[32];
+    const uint32_t t = threadIdx.x, lane = t & 31, w = t >> 5;
+    uint32_t v[kPer], sum = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+        const uint32_t i = t * kPer + k;
+        v[k] = i < kOrderBuckets ? hist[i] : 0u;
+        sum += v[k];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(kFull, incl, o);
+        if ((int)lane >= o) incl += x;
+    }
+    if (lane == 31) warp_sums[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t ws = warp_sums[lane], wi = ws;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(kFull, wi, o);
+            if ((int)lane >= o) wi += x;
+        }
+        warp_sums[lane] = wi - ws;  // exclusive prefix of the warps
+    }
+    __syncthreads();
+    uint32_t run = warp_sums[w] + incl - sum;
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+        const uint32_t i = t * kPer + k;
+        if (i < kOrderBuckets) hist[i] = run;
+        run += v[k];
+    }
+}
+
+__global__ void __launch_bounds__(256) ray_scatter_kernel(const uint32_t *__restrict__ bucket, uint32_t n,
+                                                          uint32_t *__restrict__ next, uint32_t *__restrict__ order) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint32_t pos = atomicAdd(next + bucket[r], 1u);
+    if (pos < n) order[pos] = r;
+    else flag_error(QSDVR_DEVERR_CAPACITY);
+}
+
 // Positive control of the bounds-checked build: element kBoundsProbe of a buffer declared to
 // hold kBoundsDeclared elements, which physically holds kBoundsHeld, so the write is in
 // bounds whether or not the check redirects it.
@@ -1223,6 +1303,31 @@ extern "C" int qsdvr_ray_order_keys(const qsdvr_ray_info *rays, const float *ori
     if (!(interval > 0.0f)) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_order_keys: interval must be > 0");
     ray_order_keys_kernel<<<grid_for(ray_count, 256), 256, 0, stream>>>(rays, origin, dir, ray_count, interval, keys);
     return check_launch("qsdvr_ray_order_keys");
+}
+
+extern "C" size_t qsdvr_ray_order_workspace_size(uint32_t ray_count) {
+    return ((size_t)kOrderBuckets + (size_t)ray_count) * sizeof(uint32_t);
+}
+
+extern "C" int qsdvr_ray_order(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
+                               float interval, uint32_t *order, void *workspace, size_t workspace_bytes,
+                               cudaStream_t stream) {
+    if (ray_count == 0) return QSDVR_OK;
+    if (!rays || !origin || !dir || !order)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_order: null pointer");
+    if (!(interval > 0.0f)) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_order: interval must be > 0");
+    const size_t need = qsdvr_ray_order_workspace_size(ray_count);
+    if (!workspace || workspace_bytes < need || !aligned(workspace, 4))
+        return set_error(QSDVR_ERR_WORKSPACE, "qsdvr_ray_order: workspace %zu < %zu bytes (4-byte aligned)",
+                         workspace_bytes, need);
+    uint32_t *hist = static_cast<uint32_t *>(workspace), *bucket = hist + kOrderBuckets;
+    const int st = check_cuda(cudaMemsetAsync(hist, 0, kOrderBuckets * sizeof(uint32_t), stream), "qsdvr_ray_order: memset");
+    if (st != QSDVR_OK) return st;
+    const unsigned blocks = grid_for(ray_count, 256);
+    ray_bucket_kernel<<<blocks, 256, 0, stream>>>(rays, origin, dir, ray_count, interval, bucket, hist);
+    bucket_scan_kernel<<<1, 1024, 0, stream>>>(hist);
+    ray_scatter_kernel<<<blocks, 256, 0, stream>>>(bucket, ray_count, hist, order);
+    return check_launch("qsdvr_ray_order");
 }
 
 extern "C" int qsdvr_check_bounds(float *buffer, cudaStream_t stream) {

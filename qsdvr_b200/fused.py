@@ -45,7 +45,8 @@ _lib.extra_signatures({
     "qsdvr_separable_sdf_grad": [P, U32, P, P, P, P, P],
     "qsdvr_ray_order_keys": [P, P, P, U32, F32, P, P],
     "qsdvr_sdf_cells_bf16": [P, P, ctypes.c_uint64, P],
-}, {"qsdvr_render_workspace_size": [ctypes.POINTER(RenderArgs)]})
+    "qsdvr_ray_order": [P, P, P, U32, F32, P, P, ctypes.c_size_t, P],
+}, {"qsdvr_render_workspace_size": [ctypes.POINTER(RenderArgs)], "qsdvr_ray_order_workspace_size": [U32]})
 
 _workspaces: dict = {}
 
@@ -160,15 +161,34 @@ def _stream(dev):
 
 def ray_order(rays, origin, direction, interval) -> torch.Tensor:
     """A permutation (int32 [N]) that lists the rays by the Morton code of their in-box
-    midpoint (qsdvr_ray_order_keys), rays without samples last.  Passed as ``order`` to the
-    render calls, neighbouring rays in the kernel's schedule cross neighbouring cells, so more
-    of the gathered rows and gradient lines are found in L2."""
+    midpoint on a 32^3 lattice (qsdvr_ray_order: the library's counting sort), rays without
+    samples last.  Passed as ``order`` to the render calls, neighbouring rays in the kernel's
+    schedule cross neighbouring cells, so more of the gathered rows and gradient lines are found
+    in L2."""
+    dev, n = _check_batch(rays, origin, direction)
+    order = torch.empty(n, dtype=torch.int32, device=dev)
+    if n == 0:
+        return order
+    need = int(_lib.lib().qsdvr_ray_order_workspace_size(n))
+    key = (dev, "order")
+    ws = _workspaces.get(key)
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(need, dtype=torch.uint8, device=dev)
+        _workspaces[key] = ws
+    with torch.cuda.device(dev):
+        call("qsdvr_ray_order", _ptr(rays), _ptr(origin), _ptr(direction), n, float(interval), _ptr(order),
+             ws.data_ptr(), ws.numel(), _stream(dev))
+    return order
+
+
+def ray_order_keys(rays, origin, direction, interval) -> torch.Tensor:
+    """The 30-bit Morton codes of the rays' midpoints (qsdvr_ray_order_keys), int32 [N]."""
     dev, n = _check_batch(rays, origin, direction)
     keys = torch.empty(n, dtype=torch.int32, device=dev)
     with torch.cuda.device(dev):
         call("qsdvr_ray_order_keys", _ptr(rays), _ptr(origin), _ptr(direction), n, float(interval), _ptr(keys),
              _stream(dev))
-    return torch.argsort(keys).to(torch.int32)
+    return keys
 
 
 def render_forward(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="compat",

@@ -260,10 +260,11 @@ def test_fused_sh_degree3_vs_oracle(fz, storage):
 
 
 def test_ray_order_gives_same_results(fz):
-    """Rays taken in Morton order of their midpoints (qsdvr_ray_order_keys + args.order) give
-    the same colours, loss and gradients as the batch order; the keys are the 30-bit Morton
-    codes of the midpoints (rays without samples last); an order entry outside the batch is
-    skipped and flagged, not read."""
+    """Rays taken in Morton order of their midpoints (qsdvr_ray_order, args.order) give the
+    same colours, loss and gradients as the batch order.  The order is a permutation that lists
+    the rays by the 15-bit Morton code of their midpoint (32^3 lattice; rays without samples
+    last); qsdvr_ray_order_keys gives the 30-bit codes (1024^3 lattice).  An order entry outside
+    the batch is skipped and flagged, not read."""
     import numpy as np
 
     from qsdvr_b200 import _lib, scenes
@@ -277,20 +278,26 @@ def test_ray_order_gives_same_results(fz):
     args = (cam.rayList, cam.originList, cam.dirList)
     order = fz.ray_order(*args, interval)
     assert torch.equal(order.sort().values.cpu(), torch.arange(n, dtype=torch.int32))
-    # keys: Morton code of the in-box midpoint on a 1024^3 lattice
     r, o, d = (t.cpu().numpy() for t in args)
     ns = r[:, 0].astype(np.int64)
     t = 0.5 * (ns - 1).astype(np.float32) * np.float32(interval)
     mid = o + d * t[:, None]
-    q = np.clip(np.floor((mid + 1.0) * 512.0), 0, 1023).astype(np.int64)
-    key = np.zeros(n, np.int64)
-    for b in range(10):
-        for a in range(3):
-            key |= ((q[:, a] >> b) & 1) << (3 * b + a)
-    key[ns < 2] = 0x7FFFFFFF
-    got = order.cpu().numpy()
-    ks = key[got]
-    assert np.all(np.diff(ks) >= 0) or np.mean(np.diff(ks) >= 0) > 0.999  # float rounding at lattice edges
+
+    def morton(bits, none):
+        q = np.clip(np.floor((mid + 1.0) * (1 << (bits - 1))), 0, (1 << bits) - 1).astype(np.int64)
+        key = np.zeros(n, np.int64)
+        for b in range(bits):
+            for a in range(3):
+                key |= ((q[:, a] >> b) & 1) << (3 * b + a)
+        key[ns < 2] = none
+        return key
+
+    # the order: 15-bit codes non-decreasing (float rounding at lattice edges aside)
+    ks = morton(5, 1 << 15)[order.cpu().numpy()]
+    assert np.all(np.diff(ks) >= 0) or np.mean(np.diff(ks) >= 0) > 0.999
+    # the keys entry point: 30-bit codes
+    k30 = fz.ray_order_keys(*args, interval).cpu().numpy().astype(np.int64)
+    assert np.mean(k30 == morton(10, 0x7FFFFFFF)) > 0.999
     out = []
     for o_ in (None, order):
         sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
