@@ -463,7 +463,7 @@ def _ray_matrix(rays: torch.Tensor):
     n_s = rays[:, 0]
     n_r = torch.clamp(n_s - 1, min=0)
     L = int(n_r.max()) if rays.shape[0] else 0
-    i = torch.arange(max(L, 1))
+    i = torch.arange(max(L, 1), device=rays.device)
     valid = i.unsqueeze(0) < n_r.unsqueeze(1)
     r_idx = torch.where(valid, rays[:, 3:4] + i, torch.zeros_like(valid, dtype=torch.long))
     s0 = torch.where(valid, rays[:, 1:2] + i, torch.zeros_like(valid, dtype=torch.long))
@@ -492,8 +492,8 @@ def ray_aggregate(rgb, sdf, rays, k: float, sdf_ok=None):
     w = (T * alpha).unsqueeze(-1)
     color = (w * rgb[r_idx] * valid.unsqueeze(-1)).sum(1)
     M = rgb.shape[0]
-    alpha_list = torch.zeros(M, dtype=rgb.dtype)
-    T_list = torch.zeros(M, dtype=rgb.dtype)
+    alpha_list = torch.zeros(M, dtype=rgb.dtype, device=rgb.device)
+    T_list = torch.zeros(M, dtype=rgb.dtype, device=rgb.device)
     alpha_list[r_idx[valid]] = alpha[valid].detach()
     T_list[r_idx[valid]] = T[valid].detach()
     return color, alpha_list, T_list
@@ -525,10 +525,10 @@ def ray_aggregate_backward_reference(grad, rgb, sdf, rays, alpha, T, k: float):
     zero = a == 0
     d_next = torch.where(zero, torch.zeros_like(d_next), d_next)
     d_this = torch.where(zero, torch.zeros_like(d_this), d_this)
-    sdf_grad = torch.zeros(sdf.shape[0], dtype=DTYPE)
+    sdf_grad = torch.zeros(sdf.shape[0], dtype=DTYPE, device=sdf.device)
     sdf_grad.index_add_(0, s0[valid], (dL_da * d_this)[valid])
     sdf_grad.index_add_(0, (s0 + 1)[valid], (dL_da * d_next)[valid])
-    rgb_grad = torch.zeros(rgb.shape[0], 3, dtype=DTYPE)
+    rgb_grad = torch.zeros(rgb.shape[0], 3, dtype=DTYPE, device=rgb.device)
     rgb_grad[r_idx[valid]] = (g * (Tm * a).unsqueeze(-1))[valid]
     return rgb_grad, sdf_grad
 

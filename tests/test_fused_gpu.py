@@ -477,8 +477,9 @@ def test_nonfinite_appearance_row_of_inactive_samples(fz):
     colour of each ray that reads such a row NaN; the fused kernel neither gathers nor shades
     those samples, so their rows never reach a colour or a gradient.  Here every row that some
     alpha = 0 sample reads and no alpha > 0 sample reads holds NaN (compat mode, the
-    reference's addressing): the kernel's colours and gradients equal those of the same model
-    with those rows zeroed, bit for bit, and are finite; the reference (run live when built)
+    reference's addressing): the kernel's colours equal those of the same model with those rows
+    zeroed, bit for bit, its gradients up to the order of their float atomics, and all are
+    finite; the reference (run live when built)
     gives NaN colours on the rays that read them."""
     from oracle.build_ref import load_reference
     from qsdvr_b200 import scenes
@@ -515,7 +516,8 @@ def test_nonfinite_appearance_row_of_inactive_samples(fz):
         out.append((img, loss, sg, dg))
     (i0, l0, s0, d0), (i1, l1, s1, d1) = out
     assert torch.isfinite(i0).all() and torch.isfinite(s0).all() and torch.isfinite(d0).all()
-    assert torch.equal(i0, i1) and torch.equal(s0, s1) and torch.equal(d0, d1)
+    # colours bit for bit; gradients up to the order of their float atomics
+    assert torch.equal(i0, i1) and rel_err(s0.cpu(), s1.cpu()) < 1e-6 and rel_err(d0.cpu(), d1.cpu()) < 1e-6
     ref = load_reference()
     if ref is not None:
         want, _, _ = reference_render(ref, grid7, bad, pts, R, k, target)

