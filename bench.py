@@ -350,8 +350,8 @@ def run_ours(args, cfg, device, ws, rank):
     # gradients accumulate over the steps into buffers zeroed once before timing (the
     # scatter's work does not depend on what the buffers hold); zeroing and the optimizer
     # step are timed separately below, and a full training step beside them
-    # each step takes its rays in the Morton order of their midpoints (keys + sort inside the
-    # timed step; the kernel events bracket the train launch alone)
+    # each step takes its rays in the Morton order of their midpoints (the library's counting
+    # sort inside the timed step; the kernel events bracket the train launch alone)
     def step(i, ev):
         b = batches[i % len(batches)]
         loss.zero_()
@@ -449,13 +449,14 @@ def run_ours(args, cfg, device, ws, rank):
                                f"{mode} mode, k={K_LOGISTIC}"
                                + (", same-cell merged appearance scatter" if args.merge else ""),
                    "global_batch": cfg["rays"] * ws, "samples_per_step": round(mean_samples),
-                   "step": "ray-order keys + sort (rays taken in Morton order of their midpoints), then one "
-                           "fused forward/MSE/backward launch; gradients accumulated into buffers zeroed "
-                           "before the timed region (zeroing, optimizer and full step in step_parts)",
+                   "step": "the ray order (the library's counting sort of the rays' midpoints on a 32^3 "
+                           "Morton lattice: bucket, scan and scatter kernels), then one fused forward/MSE/"
+                           "backward launch; gradients accumulated into buffers zeroed before the timed region "
+                           "(zeroing, optimizer and full step in step_parts)",
                    "l2": "inputs larger than L2 (grids 2.7 GB), no flush", "parallelism": f"replicas x{ws}"},
         "e2e": {"value": round(e2e_value, 1), "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4,
                 "wall_s": round(wall_e2e, 3)},
-        "gpu_launches": 2 * args.steps,  # qsdvr_ray_order_keys + the train kernel per step
+        "gpu_launches": 4 * args.steps,  # qsdvr_ray_order's 3 kernels + the train kernel per step
         "step_parts": step_parts,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": None if traffic is None else round(traffic),

@@ -118,7 +118,6 @@ struct Params {
     uint64_t sample_capacity;
     const uint32_t *order;  // optional: the i-th ray taken is order[i]
     bool grad_bf16;         // data_grad holds bf16 values
-    bool merge;             // samples of a chunk in the same cell send one summed RED per corner row
 };
 
 constexpr uint32_t kListT = 33;  // list sampling: 33 SDF positions, 32 render samples per ray
@@ -216,14 +215,20 @@ __device__ __forceinline__ void sep_red(float4 *sg, uint32_t R, const CellPoint 
     if (!is_zero4(z)) red4(reinterpret_cast<float *>(QSDVR_AT(sg, 2 * R + c.cz, 1, n)), z);
 }
 
-template <typename S>
+// Kernel variants (a template parameter, so each instance holds only the code it runs: the
+// kernel's code size sets how often its warps wait for instruction fetch).
+constexpr int kVarSep = 1;    // separable SDF tables instead of the dense cell grid
+constexpr int kVarMerge = 2;  // same-cell merged appearance scatter
+
+template <typename S, int kVar>
 __device__ __forceinline__ void load_cell(const Params &p, const CellPoint &c, float *a) {
-    if (p.sep) sep_cell(p.sep, p.R, c, a);
+    if constexpr ((kVar & kVarSep) != 0) sep_cell(p.sep, p.R, c, a);
     else Store<S>::cell(p.sdf, (uint32_t)c.index, a, (uint64_t)p.R * p.R * p.R);
 }
 
+template <int kVar>
 __device__ __forceinline__ void scatter_cell(const Params &p, const CellPoint &c, const float *g) {
-    if (p.sep_grad) sep_red(p.sep_grad, p.R, c, g);
+    if constexpr ((kVar & kVarSep) != 0) sep_red(p.sep_grad, p.R, c, g);
     else red_cell(p.sdf_grad, (uint32_t)c.index, g, (uint64_t)p.R * p.R * p.R);
 }
 
@@ -374,7 +379,7 @@ struct Sample {
 // Forward evaluation of render sample i = chunk*32 + lane (kernel/camera.cu:60-96,
 // kernel/surface.cu:54-115, kernel/render.cu:98-179, :239-244).  Leaves the sample's
 // interpolated 32 channels in the warp's tile.
-template <bool kCompat, typename S, int kDeg>
+template <bool kCompat, typename S, int kDeg, int kVar>
 __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3 d, uint32_t nr, uint32_t chunk,
                                            int lane, float *tile, Sample &s, const float *from_slot = nullptr,
                                            float *to_slot = nullptr) {
@@ -392,7 +397,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     float s1 = 0.0f;
     if (live) {
         if (cell_in_grid(s.c1, R)) {
-            load_cell<S>(p, s.c1, a1);
+            load_cell<S, kVar>(p, s.c1, a1);
             s1 = checked_sdf<kCompat>(a1, s.c1.u, (float)R);
         } else {
             ok = false;
@@ -404,7 +409,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
             to_cell(tl ? at_t(o, d, tl[i]) : march(o, d, (float)i, p.interval), p.volume_offset, R);
         if (cell_in_grid(c0, R)) {
             float a0[7];
-            load_cell<S>(p, c0, a0);
+            load_cell<S, kVar>(p, c0, a0);
             s0 = checked_sdf<kCompat>(a0, c0.u, (float)R);
         } else {
             ok = false;
@@ -417,7 +422,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
                    p.volume_offset, R);
     float ar[7];
     if (live && cell_in_grid(s.cr, R)) {
-        load_cell<S>(p, s.cr, ar);
+        load_cell<S, kVar>(p, s.cr, ar);
         s.nrm = sample_normal<kCompat>(ar, s.cr.u);
     } else {
         ok = false;
@@ -555,7 +560,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
 
 // Alpha only (no normal, gather or shading): what the backward-only pass needs to
 // rebuild the transmittance at each chunk start.  Validity matches eval_chunk.
-template <bool kCompat, typename S>
+template <bool kCompat, typename S, int kVar>
 __device__ __forceinline__ void eval_alpha(const Params &p, uint32_t r, f3 o, f3 d, uint32_t nr, uint32_t chunk,
                                            int lane, Sample &s) {
     const uint32_t R = p.R;
@@ -569,7 +574,7 @@ __device__ __forceinline__ void eval_alpha(const Params &p, uint32_t r, f3 o, f3
     if (live) {
         if (cell_in_grid(c1, R)) {
             float a1[7];
-            load_cell<S>(p, c1, a1);
+            load_cell<S, kVar>(p, c1, a1);
             s1 = checked_sdf<kCompat>(a1, c1.u, (float)R);
         } else {
             ok = false;
@@ -581,7 +586,7 @@ __device__ __forceinline__ void eval_alpha(const Params &p, uint32_t r, f3 o, f3
             to_cell(tl ? at_t(o, d, tl[i]) : march(o, d, (float)i, p.interval), p.volume_offset, R);
         if (cell_in_grid(c0, R)) {
             float a0[7];
-            load_cell<S>(p, c0, a0);
+            load_cell<S, kVar>(p, c0, a0);
             s0 = checked_sdf<kCompat>(a0, c0.u, (float)R);
         } else {
             ok = false;
@@ -661,20 +666,20 @@ __device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(
 
 // Scatter the data-gradient tile (rows of 32 channels per lane's sample) through the
 // trilinear weights: 8 lanes per sample, one 16-byte RED (8 bytes for a bf16 gradient) per
-// lane and corner.  With p.merge, samples of the chunk that lie in the same cell (same base
+// lane and corner.  In the kVarMerge variant, samples of the chunk that lie in the same cell (same base
 // vertex) are found with one match_any: the first of them sums the others' weighted
 // contributions (their gradient rows and weights read from the tile) and sends one RED per
 // corner row for all of them; the others send nothing.
-template <int kDeg>
+template <int kDeg, int kVar>
 __device__ __forceinline__ void scatter_tile(const Params &p, float *tile, const Sample &s, int lane) {
     using RW = Rows<kDeg>;
     constexpr int kC = RW::kC, kRow = RW::kStride, kL = RW::kLanes, kPS = RW::kPerStep;
     const uint32_t R1 = p.R + 1, sy = R1, sz = R1 * R1;
     [[maybe_unused]] const uint64_t ne = (uint64_t)kC * R1 * R1 * R1;  // gradient elements
     const int q = lane % kL;
-    uint32_t others = 0;  // p.merge: the later samples of this lane's cell, summed into this one
+    uint32_t others = 0;  // kVarMerge: the later samples of this lane's cell, summed into this one
     bool follower = false;
-    if (p.merge) {
+    if constexpr ((kVar & kVarMerge) != 0) {
         const uint32_t key = s.valid ? s.vbase : (0x80000000u | (uint32_t)lane);  // vertices < 2^31
         const uint32_t peers = __match_any_sync(kFull, key);
         follower = (peers & ((1u << lane) - 1u)) != 0;  // a lower lane of the same cell leads
@@ -687,7 +692,7 @@ __device__ __forceinline__ void scatter_tile(const Params &p, float *tile, const
 #pragma unroll 2
     for (int st = 0; st < kL; ++st) {
         const int j = st * kPS + lane / kL;
-        const uint32_t more = p.merge ? __shfl_sync(kFull, others, j) : 0u;
+        const uint32_t more = (kVar & kVarMerge) != 0 ? __shfl_sync(kFull, others, j) : 0u;
         const float4 w = ld4(tile + j * kRow + kC);
         const uint32_t vb = __float_as_uint(w.x);
         if (vb == kNoVertex) continue;
@@ -726,7 +731,7 @@ __device__ __forceinline__ void scatter_tile(const Params &p, float *tile, const
 // compositing backward (compat: the reference's Tac / (alpha - 1) form; fixed: the
 // division-free reverse affine scan), dalpha/dsdf, the quadric-cell gradients and the
 // appearance scatter.  suf and next_this carry the suffix state to the preceding chunk.
-template <bool kCompat, typename S, int kDeg>
+template <bool kCompat, typename S, int kDeg, int kVar>
 __device__ __forceinline__ void backward_chunk(const Params &p, f3 o, f3 d, uint32_t nr, uint32_t c, int lane,
                                                float *tile, const Sample &s, float T, f3 g, f3 &suf,
                                                float &next_this) {
@@ -794,7 +799,7 @@ __device__ __forceinline__ void backward_chunk(const Params &p, f3 o, f3 d, uint
         // SDF sample i+1 and, for the ray's first lane, SDF sample 0
         const float gs1 = dl * d_next + (i + 1 < nr ? from_next : 0.0f);
         float a1[7], gq[7];
-        load_cell<S>(p, s.c1, a1);
+        load_cell<S, kVar>(p, s.c1, a1);
         quad_sdf_grad(a1, s.c1.u, (float)p.R, gs1, gq);
         // rgb gradient; 0 for an unshaded sample (alpha = 0) unless the ray's colour
         // gradient is not finite (a NaN colour), which the reference spreads to
@@ -807,36 +812,36 @@ __device__ __forceinline__ void backward_chunk(const Params &p, f3 o, f3 d, uint
             const f3 gn =
                 shade_any_backward_inplace<kCompat, kDeg>(grgb, s.nrm, d, tile + lane * kRow, s.spec);
             float ar[7], gr[6];
-            load_cell<S>(p, s.cr, ar);
+            load_cell<S, kVar>(p, s.cr, ar);
             sample_normal_grad<kCompat>(ar, s.cr.u, gn, gr);
             if (s.cr.index == s.c1.index) {
 #pragma unroll
                 for (int t = 0; t < 6; ++t) gq[t] += gr[t];
-                scatter_cell(p, s.c1, gq);
+                scatter_cell<kVar>(p, s.c1, gq);
             } else {
-                scatter_cell(p, s.c1, gq);
+                scatter_cell<kVar>(p, s.c1, gq);
                 const float g7[7] = {gr[0], gr[1], gr[2], gr[3], gr[4], gr[5], 0.0f};
-                scatter_cell(p, s.cr, g7);
+                scatter_cell<kVar>(p, s.cr, g7);
             }
         } else {
             // alpha = 0: the colour's gradients (data row, normal) are 0 and the row
             // in the tile is the gather's zeros, which the scatter skips
-            scatter_cell(p, s.c1, gq);
+            scatter_cell<kVar>(p, s.c1, gq);
         }
         if (i == 0) {
             const CellPoint c0 = to_cell(march(o, d, 0.0f, p.interval), p.volume_offset, p.R);
             float a0[7], g0[7];
-            load_cell<S>(p, c0, a0);
+            load_cell<S, kVar>(p, c0, a0);
             quad_sdf_grad(a0, c0.u, (float)p.R, mine_this, g0);
-            scatter_cell(p, c0, g0);
+            scatter_cell<kVar>(p, c0, g0);
         }
     }
     __syncwarp();
-    scatter_tile<kDeg>(p, tile, s, lane);
+    scatter_tile<kDeg, kVar>(p, tile, s, lane);
     __syncwarp();
 }
 
-template <bool kCompat, typename S, int kPass, bool kLogT, int kDeg>
+template <bool kCompat, typename S, int kPass, bool kLogT, int kDeg, int kVar>
 __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kernel(const Params p) {
     constexpr int kRow = Rows<kDeg>::kStride;
     constexpr uint32_t kChunkFloats = chunk_floats<kDeg>();
@@ -897,10 +902,10 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                         if (c < 32) ts_lo = tr.carry; else ts_hi = tr.carry;
                     }
                     if (kPass == kBackward) {
-                        eval_alpha<kCompat, S>(p, r, o, d, nr, c, lane, s);
+                        eval_alpha<kCompat, S, kVar>(p, r, o, d, nr, c, lane, s);
                         tr.step(s.alpha, s.valid, lane);
                     } else {
-                        eval_chunk<kCompat, S, kDeg>(p, r, o, d, nr, c, lane, tile, s);
+                        eval_chunk<kCompat, S, kDeg, kVar>(p, r, o, d, nr, c, lane, tile, s);
                         const float T = tr.step(s.alpha, s.valid, lane);
                         if (p.sample_alpha && c * kWarp + lane < nr) {
                             const uint64_t m = (uint64_t)info.render_offset + c * kWarp + lane;
@@ -923,9 +928,9 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
             float next_this = 0.0f;    // d_this term of the first sample of the following chunk
             for (int c = (int)chunks - 1; c >= 0; --c) {
                 tr.carry = __shfl_sync(kFull, c < 32 ? ts_lo : ts_hi, c & 31);
-                eval_chunk<kCompat, S, kDeg>(p, r, o, d, nr, (uint32_t)c, lane, tile, s);
+                eval_chunk<kCompat, S, kDeg, kVar>(p, r, o, d, nr, (uint32_t)c, lane, tile, s);
                 const float T = tr.step(s.alpha, s.valid, lane);
-                backward_chunk<kCompat, S, kDeg>(p, o, d, nr, (uint32_t)c, lane, tile, s, T, g, suf, next_this);
+                backward_chunk<kCompat, S, kDeg, kVar>(p, o, d, nr, (uint32_t)c, lane, tile, s, T, g, suf, next_this);
             }
         }
         // ---------------- train: the forward chunks, the MSE gradient, then the chunks in
@@ -964,7 +969,7 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                     float *sl = (slot && c + 1 < chunks && c + 1 + kSlotChunks >= chunks)
                                     ? slot + (c % kSlotChunks) * kChunkFloats
                                     : nullptr;
-                    eval_chunk<kCompat, S, kDeg>(p, r, o, d, nr, c, lane, tile, s, fwd ? nullptr : sl,
+                    eval_chunk<kCompat, S, kDeg, kVar>(p, r, o, d, nr, c, lane, tile, s, fwd ? nullptr : sl,
                                                  fwd ? sl : nullptr);
                     T = tr.step(s.alpha, s.valid, lane);
                 } else {
@@ -984,7 +989,7 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                     acc.z += s.rgb.z * s.alpha * T;
                     __syncwarp();
                 } else {
-                    backward_chunk<kCompat, S, kDeg>(p, o, d, nr, c, lane, tile, s, T, g, suf, next_this);
+                    backward_chunk<kCompat, S, kDeg, kVar>(p, o, d, nr, c, lane, tile, s, T, g, suf, next_this);
                 }
             }
         }
@@ -996,8 +1001,20 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
 
 constexpr size_t kCounterBytes = 256;
 
-// Calls f.template run<kCompat, S, kLogT, kDeg>() for the kernel configuration of `a`
-// (degree 3 exists only in the packed, fixed-mode layout).
+// Calls f.template run<kCompat, S, kLogT, kDeg, kVar>() for the kernel configuration of `a`
+// (degree 3 exists only in the packed, fixed-mode layout; the separable SDF only with degree
+// 2 and without the merged scatter, which validate() enforces).
+template <bool C, typename S, bool L, int D, typename F>
+void with_variant(const qsdvr_render_args *a, F &f) {
+    if (a->sdf_layers) {
+        if constexpr (D == 2) f.template run<C, S, L, D, kVarSep>();
+    } else if (a->merge_scatter) {
+        f.template run<C, S, L, D, kVarMerge>();
+    } else {
+        f.template run<C, S, L, D, 0>();
+    }
+}
+
 template <typename F>
 void dispatch(const qsdvr_render_args *a, F &f) {
     const bool compat = a->mode == QSDVR_MODE_COMPAT;
@@ -1006,16 +1023,20 @@ void dispatch(const qsdvr_render_args *a, F &f) {
     const bool deg3 = a->sh_degree == 3;
     using B = __nv_bfloat16;
     if (deg3) {
-        if (bf16) { if (logt) f.template run<false, B, true, 3>(); else f.template run<false, B, false, 3>(); }
-        else { if (logt) f.template run<false, float, true, 3>(); else f.template run<false, float, false, 3>(); }
+        if (bf16) { if (logt) with_variant<false, B, true, 3>(a, f); else with_variant<false, B, false, 3>(a, f); }
+        else { if (logt) with_variant<false, float, true, 3>(a, f); else with_variant<false, float, false, 3>(a, f); }
     } else if (compat) {
-        if (bf16) { if (logt) f.template run<true, B, true, 2>(); else f.template run<true, B, false, 2>(); }
-        else { if (logt) f.template run<true, float, true, 2>(); else f.template run<true, float, false, 2>(); }
+        if (bf16) { if (logt) with_variant<true, B, true, 2>(a, f); else with_variant<true, B, false, 2>(a, f); }
+        else { if (logt) with_variant<true, float, true, 2>(a, f); else with_variant<true, float, false, 2>(a, f); }
     } else {
-        if (bf16) { if (logt) f.template run<false, B, true, 2>(); else f.template run<false, B, false, 2>(); }
-        else { if (logt) f.template run<false, float, true, 2>(); else f.template run<false, float, false, 2>(); }
+        if (bf16) { if (logt) with_variant<false, B, true, 2>(a, f); else with_variant<false, B, false, 2>(a, f); }
+        else { if (logt) with_variant<false, float, true, 2>(a, f); else with_variant<false, float, false, 2>(a, f); }
     }
 }
+
+// The forward pass scatters nothing: its merged variant is the plain one.
+template <int kPass, int kVar>
+constexpr int pass_variant() { return kPass == kForward ? (kVar & ~kVarMerge) : kVar; }
 
 // Persistent grid and workspace size for the current device: one block per resident slot
 // of the train kernel (the heaviest instantiation, which bounds the others).
@@ -1030,14 +1051,17 @@ struct Occupancy {
     int per_sm = 0, train_per_sm = 0;
     size_t chunk_bytes = 0;
     cudaError_t err = cudaSuccess;
-    template <bool C, typename S, bool L, int D>
+    template <bool C, typename S, bool L, int D, int V>
     void run() {
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&train_per_sm, render_kernel<C, S, kTrain, L, D>, kThreads, 0);
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&train_per_sm, render_kernel<C, S, kTrain, L, D, V>, kThreads,
+                                                            0);
         per_sm = train_per_sm;
         if (err == cudaSuccess && pass == kForward)
-            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<C, S, kForward, L, D>, kThreads, 0);
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, render_kernel<C, S, kForward, L, D, pass_variant<kForward, V>()>, kThreads, 0);
         if (err == cudaSuccess && pass == kBackward)
-            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<C, S, kBackward, L, D>, kThreads, 0);
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_kernel<C, S, kBackward, L, D, V>,
+                                                                kThreads, 0);
         chunk_bytes = chunk_floats<D>() * sizeof(float);
     }
 };
@@ -1072,9 +1096,9 @@ struct Launcher {
     const Params *p;
     unsigned blocks;
     cudaStream_t stream;
-    template <bool C, typename S, bool L, int D>
+    template <bool C, typename S, bool L, int D, int V>
     void run() {
-        render_kernel<C, S, kPass, L, D><<<blocks, kThreads, 0, stream>>>(*p);
+        render_kernel<C, S, kPass, L, D, pass_variant<kPass, V>()><<<blocks, kThreads, 0, stream>>>(*p);
     }
 };
 
@@ -1107,7 +1131,6 @@ int launch(const qsdvr_render_args *a, cudaStream_t stream) {
     p.sample_capacity = a->sample_capacity;
     p.order = a->order;
     p.grad_bf16 = a->data_grad_storage == QSDVR_STORAGE_BF16;
-    p.merge = a->merge_scatter != 0;
     unsigned blocks = grid_for(a->ray_count, kWarpsPerBlock);
     if (a->workspace) {
         const Layout L = layout_for(a, kPass);
@@ -1142,6 +1165,10 @@ int validate(const qsdvr_render_args *a, int pass) {
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: sh_degree %d not supported (2 or 3)", a->sh_degree);
     if (a->sh_degree == 3 && a->mode == QSDVR_MODE_COMPAT)
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: SH degree 3 exists only in fixed mode");
+    if (sep && a->sh_degree == 3)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: the separable SDF renders SH degree 2 only");
+    if (sep && a->merge_scatter)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: merge_scatter is not available with sdf_layers");
     if (a->transmittance != QSDVR_TRANSMITTANCE_PRODUCT && a->transmittance != QSDVR_TRANSMITTANCE_LOG)
         return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: bad transmittance form %d", a->transmittance);
     if (!(a->interval > 0.0f)) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "render: interval must be > 0");
