@@ -748,6 +748,31 @@ def run_proposal_frames(args, cfg, device):
             total_ms, kern_ms = time_device(step, args.steps, args.warmup, stream, clk)
         out[name] = dict(ms_per_frame=total_ms / args.steps, psnr=-10.0 * np.log10(max(mse, 1e-12)),
                          clocks=clk.summary())
+    # the brick-staged forward (TMA bricks of the appearance grid, one thread per ray) against
+    # the fused forward, both on the same frames listed tile by tile (8 x 8 pixels)
+    tiled = []
+    for cam in scenes.hemisphere_cameras(cfg["heldout"], cfg["radius"], size, size, cfg["focal"], 2.0, 6.0,
+                                         seed=a.seed + 99):
+        c = Camera(cam, interval, R, device=device)
+        c.GenerateRayPoints(torch.ones(size * size, dtype=torch.bool), order="tiles")
+        tiled.append((c.rayList, c.originList, c.dirList))
+    bricks = {}
+    diff = 0.0
+    for f in tiled:
+        diff = max(diff, float((fused.render_forward_bricks(f[0], f[1], f[2], sg, dg, R, interval, a.k)
+                                - uniform(f)).abs().max()))
+    for name, fn in (("fused_forward_tiles", uniform),
+                     ("brick_forward_tiles", lambda f: fused.render_forward_bricks(f[0], f[1], f[2], sg, dg, R,
+                                                                                   interval, a.k))):
+        def bstep(i, ev, fn=fn):
+            if ev is not None:
+                ev[0].record(stream)
+            fn(tiled[i % len(tiled)])
+            if ev is not None:
+                ev[1].record(stream)
+
+        bricks[name + "_ms"] = round(time_device(bstep, args.steps, args.warmup, stream)[0] / args.steps, 4)
+    bricks["max_abs_colour_difference"] = diff
     pixels = size * size
     value = pixels / (out["proposal"]["ms_per_frame"] / 1e3)
     plain = pixels / (out["uniform"]["ms_per_frame"] / 1e3)
@@ -768,6 +793,7 @@ def run_proposal_frames(args, cfg, device):
         "delta_psnr": round(out["uniform"]["psnr"] - out["proposal"]["psnr"], 3),
         "train_summary": {k: summary[k] for k in ("heldout_psnr_end", "ms_per_step", "peak_memory_gb")},
         "gpu_launches": 3 * args.steps, "clocks": out["proposal"]["clocks"],
+        "brick_staging": bricks,
     }
 
 

@@ -324,6 +324,15 @@ size_t qsdvr_render_workspace_size(const qsdvr_render_args *args);
  * GridInterpolation, Shader and RayAggregate forwards) fused with GenerateRayPoints
  * (kernel/camera.cu:132-147): writes color. */
 int qsdvr_render_forward(const qsdvr_render_args *args, cudaStream_t stream);
+/* Forward of a full frame with the appearance grid staged in shared memory by TMA, brick by
+ * brick (no counterpart in the reference; a prototype beside qsdvr_render_forward).  The
+ * rays should be listed tile by tile (8 x 8 pixels): each block of 64 rays marches its rays
+ * one thread per ray and, in rounds, copies one 8 x 8 x 8-vertex brick of the appearance grid
+ * (64 KB) into shared memory with cp.async.bulk.tensor, then renders every sample whose cell
+ * lies inside it.  Fixed mode, uniform march, log transmittance and 128-byte vertex rows only
+ * (bf16 SH degree 3 or fp32 degree 2); the same colours as qsdvr_render_forward up to the
+ * summation order of the log-transmittance. */
+int qsdvr_render_forward_bricks(const qsdvr_render_args *args, cudaStream_t stream);
 /* Replaces the backward chain of RenderGrid (models/render.py:27-170: RayAggregate, Shader,
  * GridInterpolation, SampleNormal, SampleSDF backwards) for a given dL/dcolor; per-sample
  * alpha and colour are recomputed, nothing per-sample is read from memory. */

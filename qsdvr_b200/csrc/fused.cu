@@ -17,12 +17,16 @@
 //   * the backward walks the chunks in reverse, carrying the suffix state, and
 //     scatters the data gradient back through the same tile with 16-byte vector REDs
 //     that cover whole vertex rows.
+#include <cuda.h>  // CUtensorMap (the driver is reached through cudaGetDriverEntryPoint)
 #include <cuda_bf16.h>
+
+#include <mutex>
 
 #include "common.cuh"
 #include "quadric.cuh"
 #include "raygen.cuh"
 #include "shading.cuh"
+#include "tcgen05.cuh"
 
 namespace qsdvr {
 
@@ -999,6 +1003,197 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
     if (kPass == kTrain && lane == 0 && sq != 0.0f) atomicAdd(p.loss, sq);
 }
 
+// ---- TMA brick staging for full frames (forward only, fixed mode, uniform march) --------
+// A frame's rays listed tile by tile (8 x 8 pixels, Camera order "tiles"): one block of 64
+// threads per tile, one thread per ray, each marching its render samples in order.  Rays of
+// a tile cross neighbouring cells at similar depths, so the appearance rows their current
+// samples need are staged in shared memory as one brick of kBrick^3 vertex rows, copied by
+// one TMA tensor load (cp.async.bulk.tensor.4d, this GPU's grid only, no multicast) per
+// round.  A round places the brick at the lowest corner of the tile's next samples, pulled
+// toward the lowest-numbered ray that still marches so that it always advances; each thread
+// then renders its samples while their cells stay inside the brick.  Per sample the arithmetic
+// is the fused forward's (same cell validity, alpha, interpolation order and shading), with the
+// compensated log-transmittance summed sample by sample.
+constexpr int kBrick = 8;          // vertex rows per axis: a brick covers 7 cells per axis
+constexpr int kBrickThreads = 64;  // rays per tile
+
+template <typename S, int kDeg>
+__global__ void __launch_bounds__(kBrickThreads) brick_frame_kernel(const __grid_constant__ CUtensorMap tmap,
+                                                                    const Params p) {
+    constexpr int kC = ShLayout<kDeg>::kChannels;
+    constexpr int kRowBytes = kC * (int)sizeof(S);
+    static_assert(kRowBytes == 128, "brick rows are 128-byte vertex rows");
+    constexpr uint32_t kBrickBytes = kBrick * kBrick * kBrick * kRowBytes;
+    constexpr int kPitch = kC + 1;  // per-thread row stride in floats (scalar reads conflict-free)
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // the brick at a 128-byte boundary of the dynamic shared memory (128 bytes of slack)
+    unsigned char *smem = smem_raw + ((128u - (tc::smem_addr(smem_raw) & 127u)) & 127u);
+    const S *brick = reinterpret_cast<const S *>(smem);
+    float *row = reinterpret_cast<float *>(smem + kBrickBytes) + threadIdx.x * kPitch;
+    __shared__ uint64_t mbar;
+    __shared__ int box[7];  // min x, y, z, then the leader's cell x, y, z, then the leader thread
+    const int t = threadIdx.x;
+    const uint32_t R = p.R;
+    const uint32_t r = blockIdx.x * kBrickThreads + t;
+    // this thread's ray
+    uint32_t nr = 0, i = 0;
+    f3 o{0.0f, 0.0f, 0.0f}, d{0.0f, 0.0f, 1.0f};
+    float s_prev = 0.0f, carry = 0.0f, comp = 0.0f;
+    bool in_prev = false;
+    f3 acc{0.0f, 0.0f, 0.0f};
+    if (r < p.n) {
+        const qsdvr_ray_info info = *QSDVR_AT(p.rays, r, 1, p.n);
+        nr = info.sdf_count > 1 ? info.sdf_count - 1 : 0;
+        o = load3(QSDVR_AT(p.origin, 3ull * r, 3, 3ull * p.n));
+        d = load3(QSDVR_AT(p.dir, 3ull * r, 3, 3ull * p.n));
+        if (nr > 0) {  // SDF sample 0
+            const CellPoint c0 = to_cell(march(o, d, 0.0f, p.interval), p.volume_offset, R);
+            in_prev = cell_in_grid(c0, R);
+            if (in_prev) {
+                float a0[7];
+                load_cell<S, 0>(p, c0, a0);
+                s_prev = checked_sdf<false>(a0, c0.u, (float)R);
+            }
+        }
+    }
+    if (t == 0) tc::mbar_init(&mbar, 1);
+    __syncthreads();
+    uint32_t parity = 0;
+    bool failed = false;
+    for (;;) {
+        // the cell of this thread's next render sample
+        CellPoint cr{};
+        const bool active = i < nr;
+        if (active) cr = to_cell(midpoint(o, d, i, p.interval), p.volume_offset, R);
+        if (t == 0) {
+            box[0] = box[1] = box[2] = 0x7fffffff;
+            box[6] = kBrickThreads;
+        }
+        __syncthreads();
+        if (active) {
+            atomicMin(&box[0], cr.cx);
+            atomicMin(&box[1], cr.cy);
+            atomicMin(&box[2], cr.cz);
+            atomicMin(&box[6], t);
+        }
+        __syncthreads();
+        if (box[6] == kBrickThreads) break;  // every ray of the tile is done
+        if (t == box[6]) {
+            box[3] = cr.cx;
+            box[4] = cr.cy;
+            box[5] = cr.cz;
+        }
+        __syncthreads();
+        int org[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) org[a] = min(max(box[a], box[3 + a] - (kBrick - 2)), box[3 + a]);
+        if (t == 0) {
+            // the previous round's reads of the brick are ordered before this copy by the
+            // barriers above; the copy lands through the async proxy
+            tc::fence_smem_to_async();
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_addr(&mbar)),
+                         "r"(kBrickBytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+                "%5}], [%6];" ::"r"(tc::smem_addr(smem)),
+                "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(0), "r"(org[0]), "r"(org[1]), "r"(org[2]),
+                "r"(tc::smem_addr(&mbar))
+                : "memory");
+        }
+        if (!tc::mbar_wait(&mbar, parity, 1u << 30)) {
+            if (t == 0) flag_error(QSDVR_DEVERR_TIMEOUT);
+            failed = true;
+        }
+        if (__syncthreads_or(failed)) {
+            tc::mbar_wait(&mbar, parity, 1u << 30);  // one more bounded wait for the copy in flight
+            break;
+        }
+        parity ^= 1u;
+        // render this thread's samples while their cell stays inside the brick
+        while (i < nr) {
+            cr = to_cell(midpoint(o, d, i, p.interval), p.volume_offset, R);
+            const int lx = cr.cx - org[0], ly = cr.cy - org[1], lz = cr.cz - org[2];
+            if (lx < 0 || ly < 0 || lz < 0 || lx > kBrick - 2 || ly > kBrick - 2 || lz > kBrick - 2) break;
+            // SDF sample i + 1 and the interval's validity (eval_chunk, fixed mode)
+            const CellPoint c1 = to_cell(march(o, d, (float)(i + 1), p.interval), p.volume_offset, R);
+            bool ok = in_prev;
+            float s1 = 0.0f;
+            const bool in1 = cell_in_grid(c1, R);
+            if (in1) {
+                float a1[7];
+                load_cell<S, 0>(p, c1, a1);
+                s1 = checked_sdf<false>(a1, c1.u, (float)R);
+            } else {
+                ok = false;
+            }
+            f3 nrm{0.0f, 0.0f, 1.0f};
+            if (cell_in_grid(cr, R)) {
+                float ar[7];
+                load_cell<S, 0>(p, cr, ar);
+                nrm = sample_normal<false>(ar, cr.u);
+            } else {
+                ok = false;
+            }
+            if (!ok) flag_error(QSDVR_DEVERR_INDEX);
+            if (!(isfinite(s_prev) && isfinite(s1))) ok = false;
+            const float alpha = ok ? interval_alpha<false>(alpha_term<false>(p.k, s_prev), alpha_term<false>(p.k, s1))
+                                   : 0.0f;
+            const bool shaded = ok && (alpha != 0.0f || !(isfinite(nrm.x) && isfinite(nrm.y) && isfinite(nrm.z)));
+            f3 rgb{0.0f, 0.0f, 0.0f};
+            if (shaded) {
+                // trilinear interpolation from the brick, corner order and FMA order of the
+                // fused forward's gather
+                float w[8];
+                corner_weights((cr.u.x + 1.0f) / 2.0f, (cr.u.y + 1.0f) / 2.0f, (cr.u.z + 1.0f) / 2.0f, w);
+                const int base = (lz * kBrick + ly) * kBrick + lx;
+                const int off[8] = {0, 1, kBrick, kBrick + 1, kBrick * kBrick, kBrick * kBrick + 1,
+                                    kBrick * kBrick + kBrick, kBrick * kBrick + kBrick + 1};
+                for (int ch = 0; ch < kC; ch += 8) {
+                    float v[8];
+                    if constexpr (sizeof(S) == 2) {
+                        first_bf8(*reinterpret_cast<const uint4 *>(brick + (base + off[0]) * kC + ch), w[0], v);
+#pragma unroll
+                        for (int q = 1; q < 8; ++q)
+                            fma_bf8(*reinterpret_cast<const uint4 *>(brick + (base + off[q]) * kC + ch), w[q], v);
+                    } else {
+                        const float *b0 = reinterpret_cast<const float *>(brick) + (base + off[0]) * kC + ch;
+                        float4 lo = scale4(ld4(b0), w[0]), hi = scale4(ld4(b0 + 4), w[0]);
+#pragma unroll
+                        for (int q = 1; q < 8; ++q) {
+                            const float *bq = reinterpret_cast<const float *>(brick) + (base + off[q]) * kC + ch;
+                            fma4(lo, ld4(bq), w[q]);
+                            fma4(hi, ld4(bq + 4), w[q]);
+                        }
+                        v[0] = lo.x; v[1] = lo.y; v[2] = lo.z; v[3] = lo.w;
+                        v[4] = hi.x; v[5] = hi.y; v[6] = hi.z; v[7] = hi.w;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) row[ch + q] = v[q];
+                }
+                f3 spec;
+                rgb = shade_any<false, kDeg>(nrm, d, row, &spec);
+            }
+            // compensated log-transmittance, sample by sample
+            const float T = expf(carry);
+            acc.x += rgb.x * alpha * T;
+            acc.y += rgb.y * alpha * T;
+            acc.z += rgb.z * alpha * T;
+            if (ok) {
+                const float y = log1pf(-alpha) - comp;
+                const float tt = carry + y;
+                comp = isfinite(tt) ? (tt - carry) - y : 0.0f;
+                carry = tt;
+            }
+            s_prev = s1;
+            in_prev = in1;
+            ++i;
+        }
+        __syncthreads();  // every read of this brick is done before the next copy overwrites it
+    }
+    if (r < p.n) store3(QSDVR_AT(p.color, 3ull * r, 3, 3ull * p.n), acc);
+}
+
 constexpr size_t kCounterBytes = 256;
 
 // Calls f.template run<kCompat, S, kLogT, kDeg, kVar>() for the kernel configuration of `a`
@@ -1355,6 +1550,84 @@ extern "C" int qsdvr_ray_order(const qsdvr_ray_info *rays, const float *origin, 
     bucket_scan_kernel<<<1, 1024, 0, stream>>>(hist);
     ray_scatter_kernel<<<blocks, 256, 0, stream>>>(bucket, ray_count, hist, order);
     return check_launch("qsdvr_ray_order");
+}
+
+namespace {
+
+using TensorMapEncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                            const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                            CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                            CUtensorMapFloatOOBfill);
+
+TensorMapEncodeTiledFn tensor_map_encoder(int *status) {
+    static TensorMapEncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    static cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        err = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q);
+        if (err == cudaSuccess && q == cudaDriverEntryPointSuccess) fn = reinterpret_cast<TensorMapEncodeTiledFn>(f);
+    });
+    *status = err != cudaSuccess ? check_cuda(err, "render bricks: cudaGetDriverEntryPoint")
+                                 : (fn ? QSDVR_OK : set_error(QSDVR_ERR_UNSUPPORTED, "render bricks: no cuTensorMapEncodeTiled"));
+    return fn;
+}
+
+template <typename S, int kDeg>
+int launch_bricks(const qsdvr_render_args *a, cudaStream_t stream) {
+    constexpr int kC = ShLayout<kDeg>::kChannels;
+    int st = QSDVR_OK;
+    TensorMapEncodeTiledFn encode = tensor_map_encoder(&st);
+    if (st != QSDVR_OK) return st;
+    const cuuint64_t R1 = a->reso + 1ull;
+    const cuuint64_t dims[4] = {(cuuint64_t)kC, R1, R1, R1};
+    const cuuint64_t strides[3] = {128ull, 128ull * R1, 128ull * R1 * R1};  // bytes, dims 1..3
+    const cuuint32_t box[4] = {(cuuint32_t)kC, kBrick, kBrick, kBrick};
+    const cuuint32_t estride[4] = {1, 1, 1, 1};
+    CUtensorMap tmap;
+    const CUresult cr = encode(&tmap, sizeof(S) == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                               4, const_cast<void *>(a->data), dims, strides, box, estride,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return set_error(QSDVR_ERR_CUDA, "render bricks: cuTensorMapEncodeTiled failed (%d)", (int)cr);
+    Params p{};
+    p.rays = a->rays;
+    p.origin = a->origin;
+    p.dir = a->dir;
+    p.n = a->ray_count;
+    p.R = a->reso;
+    p.interval = a->interval;
+    p.k = a->logistic_coef;
+    p.volume_offset = (float)a->reso / 2.0f;
+    p.sdf = a->sdf_grid;
+    p.data = a->data;
+    p.color = a->color;
+    const size_t smem = (size_t)kBrick * kBrick * kBrick * 128 + (size_t)kBrickThreads * (kC + 1) * sizeof(float) + 128;
+    st = check_cuda(cudaFuncSetAttribute(brick_frame_kernel<S, kDeg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem),
+                    "render bricks: shared memory");
+    if (st != QSDVR_OK) return st;
+    brick_frame_kernel<S, kDeg><<<grid_for(a->ray_count, kBrickThreads), kBrickThreads, smem, stream>>>(tmap, p);
+    return check_launch("qsdvr_render_forward_bricks");
+}
+
+}  // namespace
+
+extern "C" int qsdvr_render_forward_bricks(const qsdvr_render_args *args, cudaStream_t stream) {
+    int st = validate(args, kForward);
+    if (st != QSDVR_OK || args->ray_count == 0) return st;
+    if (args->mode != QSDVR_MODE_FIXED || args->tlist || args->sdf_layers || args->sample_alpha)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT,
+                         "qsdvr_render_forward_bricks: fixed mode, uniform march and a dense SDF grid only");
+    if (args->transmittance != QSDVR_TRANSMITTANCE_LOG)
+        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_render_forward_bricks: log transmittance only");
+    const bool bf16 = args->storage == QSDVR_STORAGE_BF16;
+    const int deg = args->sh_degree == 3 ? 3 : 2;
+    if (bf16 && deg == 3) return launch_bricks<__nv_bfloat16, 3>(args, stream);
+    if (!bf16 && deg == 2) return launch_bricks<float, 2>(args, stream);
+    return set_error(QSDVR_ERR_INVALID_ARGUMENT,
+                     "qsdvr_render_forward_bricks: 128-byte vertex rows only (bf16 SH degree 3 or fp32 degree 2)");
 }
 
 extern "C" int qsdvr_check_bounds(float *buffer, cudaStream_t stream) {

@@ -46,6 +46,7 @@ _lib.extra_signatures({
     "qsdvr_ray_order_keys": [P, P, P, U32, F32, P, P],
     "qsdvr_sdf_cells_bf16": [P, P, ctypes.c_uint64, P],
     "qsdvr_ray_order": [P, P, P, U32, F32, P, P, ctypes.c_size_t, P],
+    "qsdvr_render_forward_bricks": [ctypes.POINTER(RenderArgs), P],
 }, {"qsdvr_render_workspace_size": [ctypes.POINTER(RenderArgs)], "qsdvr_ray_order_workspace_size": [U32]})
 
 _workspaces: dict = {}
@@ -206,6 +207,22 @@ def render_forward(rays, origin, direction, sdf_grid, data, reso, interval, k, m
                   persistent=persistent, tlist=tlist, sample_alpha=sample_alpha, sdf_layers=sdf_layers, order=order)
     with torch.cuda.device(dev):
         call("qsdvr_render_forward", ctypes.byref(a), _stream(dev))
+    return color
+
+
+def render_forward_bricks(rays, origin, direction, sdf_grid, data, reso, interval, k, color=None):
+    """Colour of every ray [N,3] by the brick-staged frame forward (qsdvr_render_forward_bricks:
+    fixed mode, uniform march, log transmittance; 128-byte vertex rows, i.e. bf16 SH degree 3
+    or fp32 degree 2).  Meant for a frame's rays listed tile by tile (8 x 8 pixels,
+    ``Camera.GenerateRayPoints(order="tiles")``): each block of 64 rays shares one staged brick
+    of the appearance grid per round."""
+    dev, n = _check_batch(rays, origin, direction)
+    if color is None:
+        color = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    a = make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, "fixed", "log", color=color,
+                  persistent=False)
+    with torch.cuda.device(dev):
+        call("qsdvr_render_forward_bricks", ctypes.byref(a), _stream(dev))
     return color
 
 

@@ -522,3 +522,28 @@ def test_nonfinite_appearance_row_of_inactive_samples(fz):
     if ref is not None:
         want, _, _ = reference_render(ref, grid7, bad, pts, R, k, target)
         assert (~torch.isfinite(want)).any()  # the reference's colours on those rays are NaN
+
+
+@pytest.mark.parametrize("storage,sh", [("f32", 2), ("bf16", 3)])
+def test_brick_staged_frame_forward(fz, storage, sh):
+    """qsdvr_render_forward_bricks (TMA-staged appearance bricks, one thread per ray, rays in
+    8 x 8 tiles) gives the fused forward's colours (fixed mode, log transmittance) within 1e-5,
+    for rays in tile order and in pixel order (fewer rays per brick, same result)."""
+    from qsdvr_b200 import _lib, scenes
+    from qsdvr_b200.camera import Camera
+
+    R, k, interval = 24, 8.0, 4.0 / 160
+    grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.55, 0.01, seed=41).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=41, sh_degree=sh).to(DEV)
+    if storage == "bf16":
+        grid8, data = fz.sdf_cells_bf16(grid8), data.to(torch.bfloat16)
+    args = scenes.look_at((-1.7, 3.1, 1.9), 64, 48, 60.0, 2.0, 6.0)
+    _lib.device_error()
+    for order in ("tiles", "pixels"):
+        cam = Camera(args, interval, R)
+        cam.GenerateRayPoints(torch.ones(64 * 48, dtype=torch.bool), order=order)
+        want = fz.render_forward(cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k, "fixed", "log")
+        got = fz.render_forward_bricks(cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k)
+        assert (got - want).abs().max().item() < 1e-5, order
+        assert float(want.abs().max()) > 0.05  # the frame is not empty
+    assert _lib.device_error() == 0
