@@ -65,6 +65,12 @@ WORKLOADS = {
     # 256^3 scene: proposal path against the uniform march, rays/s and held-out PSNR
     "train512": dict(R=256, rays=65536, views=100, size=800, focal=1111.1, radius=4.03, interval=4.0 / 512,
                      storage="f32"),
+    # small cases of the proposal kernels and of the frame forwards, sized for profiler captures
+    # (a few GB on the device): the same kernels as mlp256 and proposal384 on a 128^3 grid
+    "mlp128": dict(R=128, rays=65536, views=4, size=800, focal=1111.1, radius=4.03, interval=4.0 / 256,
+                   storage="f32", online_steps=50),
+    "proposal128": dict(R=128, rays=16384, views=20, size=400, focal=555.55, radius=4.03, interval=4.0 / 512,
+                        storage="bf16", sh=3, train_steps=50, heldout=1),
     # the reference's small CPU-runnable case: a 64^3 noisy sphere, one 100x100 view at radius 4
     # (focal 138.9), 64 samples/ray, every pixel's ray, MSE against a seeded U(0,1) image
     "config1": dict(R=64, rays=10000, views=1, size=100, focal=138.9, radius=4.0, interval=4.0 / 64,
@@ -782,7 +788,7 @@ def run_proposal_frames(args, cfg, device):
         "ms_per_step": round(out["proposal"]["ms_per_frame"], 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16 storage, f32 math; MLP bf16 with f32 accumulation",
         "data": "synthetic (seeded procedural scene; model trained from a sphere init)",
-        "config": {"workload": f"proposal384: R={R}^3 BF16 SH3 model after {a.steps} training steps "
+        "config": {"workload": f"{args.workload}: R={R}^3 BF16 SH3 model after {a.steps} training steps "
                                f"({a.rays} rays/step, uniform 512 march, proposal network trained online), "
                                f"{cfg['heldout']} held-out {size}^2 frames, k={a.k}",
                    "global_batch": pixels, "step": "one full frame (all pixels, hit or not)",
@@ -971,11 +977,11 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=device)
     try:
-        if args.workload in ("proposal384", "mlp256", "train512"):
+        if args.workload in ("proposal384", "proposal128", "mlp256", "mlp128", "train512"):
             if ws > 1:
                 raise SystemExit(f"{args.workload} is a single-GPU workload")
-            fn = {"proposal384": run_proposal_frames, "mlp256": run_mlp_kernels,
-                  "train512": run_train512}[args.workload]
+            fn = {"proposal384": run_proposal_frames, "proposal128": run_proposal_frames, "mlp256": run_mlp_kernels,
+                  "mlp128": run_mlp_kernels, "train512": run_train512}[args.workload]
             print(json.dumps(fn(args, cfg, device)))
             return
         out = run_ours(args, cfg, device, ws, rank)
