@@ -464,7 +464,7 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     if (from_slot) {
         // rows stashed by the forward, one row per kL lanes per warp instruction
         const uint64_t pol = evict_last_policy();
-#pragma unroll
+#pragma unroll 2
         for (int st = 0; st < kL; ++st) {
             const int j = st * kPS + lane / kL;
             st4(tile + j * kRow + 4 * q, ld4_keep(from_slot + j * kC + 4 * q, pol));
@@ -693,7 +693,9 @@ __device__ __forceinline__ void scatter_tile(const Params &p, float *tile, const
     st4(tile + lane * kRow + kC,
         make_float4(__uint_as_float(s.valid && !follower ? s.vbase : kNoVertex), s.wx, s.wy, s.wz));
     __syncwarp();
-#pragma unroll 2
+// (one step per iteration: the REDs do not wait, and a smaller loop body keeps the kernel's
+// code small; measured as fast as two steps per iteration)
+#pragma unroll 1
     for (int st = 0; st < kL; ++st) {
         const int j = st * kPS + lane / kL;
         const uint32_t more = (kVar & kVarMerge) != 0 ? __shfl_sync(kFull, others, j) : 0u;
