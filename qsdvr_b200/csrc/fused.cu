@@ -74,6 +74,9 @@ enum Pass { kForward = 0, kBackward = 1, kTrain = 2 };
 #define QSDVR_SLOT_CHUNKS 5
 #endif
 constexpr uint32_t kSlotChunks = QSDVR_SLOT_CHUNKS;
+#ifndef QSDVR_STASH_DISCARD
+#define QSDVR_STASH_DISCARD 1
+#endif
 template <int kDeg>
 __host__ __device__ constexpr uint32_t chunk_floats() { return kWarp * Rows<kDeg>::kC; }  // rows of one chunk
 
@@ -469,6 +472,15 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
             const int j = st * kPS + lane / kL;
             st4(tile + j * kRow + 4 * q, ld4_keep(from_slot + j * kC + 4 * q, pol));
         }
+#if QSDVR_STASH_DISCARD
+        // The stash is dead once read: drop its L2 lines without writing them back (they
+        // would otherwise reach DRAM as dirty evictions) and free the room for the gathers.
+        // The tile stores above consumed every loaded value, so the loads are complete.
+        __syncwarp();
+        constexpr uint32_t kLines = kWarp * kC * sizeof(float) / 128;  // the chunk's 128-byte lines
+        for (uint32_t l = lane; l < kLines; l += kWarp)
+            asm volatile("discard.global.L2 [%0], 128;" ::"l"(from_slot + l * (128 / sizeof(float))) : "memory");
+#endif
     } else if constexpr (sizeof(S) == 2) {
         // bf16 storage: groups of kGL lanes fetch one sample's 8 corner rows as 16-byte
         // (bf16 x 8) loads, kGPS samples per step; each lane stages 8 interpolated channels
