@@ -226,9 +226,9 @@ enum {
  * per-ray tables (RayCut output after masking: RayInfo, origin = first in-box sample,
  * unit direction); samples are generated on the fly exactly as GenerateRayPoints
  * (kernel/camera.cu:60-96) would.  Only sdf_count of each record is read.  A ray with more
- * than 2048 render samples (64 warp chunks of 32) is skipped before any access: colour 0, no
+ * than 8192 render samples (256 warp chunks of 32) is skipped before any access: colour 0, no
  * gradient, QSDVR_DEVERR_RAY set.  The volume's diagonal is 2 sqrt(3), so only intervals
- * below about 0.0017 can produce such a ray (the reference marches any length).
+ * below about 0.00042 can produce such a ray (the reference marches any length).
  *   sdf_grid: [R^3][8] (a0..a6 + one pad) in `storage` precision, cell x + yR + zR^2;
  *             bf16 cells are read as (a0..a5, slot 6 + slot 7), see qsdvr_sdf_cells_bf16;
  *   data:     [(R+1)^3][C] appearance rows in `storage` precision, C = 32 (SH degree 2)

@@ -58,7 +58,7 @@ struct Rows {
     static constexpr int kLanes = kC / 4;
     static constexpr int kPerStep = kWarp / kLanes;
 };
-constexpr uint32_t kMaxChunks = 64;  // render samples per ray <= 2048
+constexpr uint32_t kMaxChunks = 256;  // render samples per ray <= 8192
 // Each staged tile row carries 4 floats of padding (the row stride keeps the row-wise and
 // lane-wise float4 accesses bank-conflict free); the gather and the scatter keep there the
 // sample's (base vertex, wx, wy, wz), the vertex kNoVertex for a sample without a row, so a
@@ -864,6 +864,8 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
     constexpr int kRow = Rows<kDeg>::kStride;
     constexpr uint32_t kChunkFloats = chunk_floats<kDeg>();
     __shared__ __align__(16) float tiles[kWarpsPerBlock][kWarp * kRow];
+    // the transmittance carry at each chunk start of the current ray, for the backward
+    __shared__ float carries[kWarpsPerBlock][kMaxChunks];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     float *tile = tiles[w];
     const uint32_t warp_id = blockIdx.x * kWarpsPerBlock + w;
@@ -909,16 +911,14 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
         }
         Sample s;
         Transmittance<kLogT> tr;
-        float ts_lo = 0.0f, ts_hi = 0.0f;  // transmittance carry at the start of chunk lane / lane+32
+        float *carry_at = carries[w];  // carry_at[c]: the transmittance carry at the start of chunk c
         float T_last = 0.0f;               // transmittance of this lane's sample in the last chunk
         // ---------------- forward (forward and backward-only passes)
         if (kPass == kForward || (kPass == kBackward && run)) {
             if (run) {
                 f3 acc{0.0f, 0.0f, 0.0f};
                 for (uint32_t c = 0; c < chunks; ++c) {
-                    if ((c & 31) == (uint32_t)lane) {
-                        if (c < 32) ts_lo = tr.carry; else ts_hi = tr.carry;
-                    }
+                    if (lane == 0) carry_at[c] = tr.carry;  // warp-uniform
                     if (kPass == kBackward) {
                         eval_alpha<kCompat, S, kVar>(p, r, o, d, nr, c, lane, s);
                         tr.step(s.alpha, s.valid, lane);
@@ -945,7 +945,8 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
             f3 suf{0.0f, 0.0f, 0.0f};  // compat: sum_{m>chunk} T a c ; fixed: R after the chunk
             float next_this = 0.0f;    // d_this term of the first sample of the following chunk
             for (int c = (int)chunks - 1; c >= 0; --c) {
-                tr.carry = __shfl_sync(kFull, c < 32 ? ts_lo : ts_hi, c & 31);
+                __syncwarp();
+                tr.carry = carry_at[c];
                 eval_chunk<kCompat, S, kDeg, kVar>(p, r, o, d, nr, (uint32_t)c, lane, tile, s);
                 const float T = tr.step(s.alpha, s.valid, lane);
                 backward_chunk<kCompat, S, kDeg, kVar>(p, o, d, nr, (uint32_t)c, lane, tile, s, T, g, suf, next_this);
@@ -978,11 +979,10 @@ __global__ void __launch_bounds__(kThreads, QSDVR_FUSED_MIN_BLOCKS) render_kerne
                 float T;
                 if (fwd || c + 1 < chunks) {
                     if (fwd) {
-                        if ((c & 31) == (uint32_t)lane) {
-                            if (c < 32) ts_lo = tr.carry; else ts_hi = tr.carry;
-                        }
+                        if (lane == 0) carry_at[c] = tr.carry;  // warp-uniform
                     } else {
-                        tr.carry = __shfl_sync(kFull, c < 32 ? ts_lo : ts_hi, c & 31);
+                        __syncwarp();
+                        tr.carry = carry_at[c];
                     }
                     float *sl = (slot && c + 1 < chunks && c + 1 + kSlotChunks >= chunks)
                                     ? slot + (c % kSlotChunks) * kChunkFloats

@@ -350,7 +350,7 @@ def test_edge_batches(fz):
 
     * An empty batch launches nothing: empty colours, zero loss, gradients untouched.
     * Rays whose record holds 0 or 1 SDF samples render black and add no gradient.
-    * A ray longer than the 2048 render samples (64 warp chunks) the fused kernels take is
+    * A ray longer than the 8192 render samples (256 warp chunks) the fused kernels take is
       skipped before any access and flagged (QSDVR_DEVERR_RAY), rendering black.
     The other rays of the batch render and train exactly as in a batch without those three."""
     from qsdvr_b200 import _lib, scenes
@@ -377,7 +377,7 @@ def test_edge_batches(fz):
     keep = torch.ones(n, dtype=torch.bool)
     keep[odd] = False
     mod = rays.clone()
-    mod[odd, 0] = torch.tensor([0, 1, 2100], dtype=torch.int32, device=DEV)
+    mod[odd, 0] = torch.tensor([0, 1, 9000], dtype=torch.int32, device=DEV)
 
     def train(r, o, d, t):
         sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
@@ -547,3 +547,29 @@ def test_brick_staged_frame_forward(fz, storage, sh):
         assert (got - want).abs().max().item() < 1e-5, order
         assert float(want.abs().max()) > 0.05  # the frame is not empty
     assert _lib.device_error() == 0
+
+
+def test_long_rays(fz):
+    """Rays of ~3000 render samples (interval 2 sqrt(3) / 3500 through a 16^3 grid: ~94 warp
+    chunks, beyond the 64 chunks of the earlier limit) train like the float64 oracle: image
+    within 1e-5, gradients within 1e-4 relative; the persistent kernel's stash then covers only
+    the last 6 chunks, and the rest are gathered again in the backward."""
+    import math
+
+    from qsdvr_b200 import _lib, scenes
+
+    R, k, interval = 16, 6.0, 2.0 * math.sqrt(3.0) / 3500
+    cam = camera_batch((2.6, -2.2, 1.9), 8, 9.0, interval, R)
+    assert int(cam.rayList[:, 0].max()) > 2048
+    grid8 = fz.pad_grid7(scenes.sphere_grid(R, 0.5, 0.01, seed=17).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=17).to(DEV)
+    target = torch.rand((cam.rayList.shape[0], 3), generator=torch.Generator().manual_seed(18)).to(DEV)
+    _lib.device_error()
+    sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+    img, _ = fz.render_train(target, cam.rayList, cam.originList, cam.dirList, grid8, data, R, interval, k, sg, dg,
+                             mode="fixed")
+    assert _lib.device_error() == 0
+    want, wg, wd = oracle_render(grid8, data, cam, R, k, compat=False, target=target)
+    assert (img.cpu().double() - want).abs().max().item() < IMG_TOL
+    assert rel_err(sg[:, :7].cpu(), wg) < GRAD_TOL
+    assert rel_err(dg.cpu(), wd) < GRAD_TOL
