@@ -645,6 +645,13 @@ def run_mlp_kernels(args, cfg, device):
                                                                   interval, k)),
         "list_train_ms": timed(lambda: fused.render_train(tg, r, o, d, sdf, data, R, interval, k, sg, dg, "fixed",
                                                           tlist=tl)),
+        # rays taken by the Morton order of their median fine sample (qsdvr_ray_order_list, as
+        # in training), the order computed inside the timed launch sequence
+        "list_train_ordered_ms": timed(lambda: fused.render_train(
+            tg, r, o, d, sdf, data, R, interval, k, sg, dg, "fixed", tlist=tl,
+            order=fused.ray_order(r, o, d, interval, tlist=tl))),
+        "uniform_train_ordered_ms": timed(lambda: fused.render_train(
+            tg, r, o, d, sdf, data, R, interval, k, sg, dg, "fixed", order=fused.ray_order(r, o, d, interval))),
         "uniform_train_ms": timed(lambda: fused.render_train(tg, r, o, d, sdf, data, R, interval, k, sg, dg,
                                                              "fixed")),
         "list_forward_ms": timed(lambda: fused.render_forward(r, o, d, sdf, data, R, interval, k, "fixed",

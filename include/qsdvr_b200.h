@@ -303,6 +303,16 @@ size_t qsdvr_ray_order_workspace_size(uint32_t ray_count);
 int qsdvr_ray_order(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
                     float interval, uint32_t *order, void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
+/* The same counting sort for list-mode batches (no counterpart in the reference): each ray is
+ * keyed on the point at its median SDF position, tlist[33 r + 16] of the [ray_count][33]
+ * sample list that qsdvr_render_* takes (args.tlist), instead of its in-box midpoint.  The
+ * proposal samples sit where the compositing weights are, so rays taken in this order run
+ * beside the rays that hit the same patch of the surface.  Same workspace as
+ * qsdvr_ray_order. */
+int qsdvr_ray_order_list(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
+                         const float *tlist, uint32_t *order, void *workspace, size_t workspace_bytes,
+                         cudaStream_t stream);
+
 /* Separable SDF for the fused renderer (the RenderGrid model's parametrisation,
  * models/render.py:172-207, without materialising [R^3][7]; LayerToGridForward,
  * kernel/surface.cu:148-229, computes the same cells): per-axis recurrence tables

@@ -77,6 +77,14 @@ constexpr uint32_t kSlotChunks = QSDVR_SLOT_CHUNKS;
 #ifndef QSDVR_STASH_DISCARD
 #define QSDVR_STASH_DISCARD 1
 #endif
+// Latency: the gather walks a chunk's samples a few at a time, and each round of its loads
+// waited for DRAM.  With QSDVR_GATHER_PREFETCH every shaded sample beyond the first round
+// requests its 8 corner rows into L2 (four bulk prefetches of two adjacent rows) as soon as
+// the chunk's alpha is known, so the later rounds find them there: SH degree 2 only (1, the
+// default: with 64-channel rows the prefetches measured slower), every degree (2), none (0).
+#ifndef QSDVR_GATHER_PREFETCH
+#define QSDVR_GATHER_PREFETCH 1
+#endif
 template <int kDeg>
 __host__ __device__ constexpr uint32_t chunk_floats() { return kWarp * Rows<kDeg>::kC; }  // rows of one chunk
 
@@ -91,13 +99,17 @@ __device__ __forceinline__ void st4_keep(float *p, float4 v, uint64_t pol) {
                  "f"(v.z), "f"(v.w), "l"(pol)
                  : "memory");
 }
-__device__ __forceinline__ float4 ld4_keep(const float *p, uint64_t pol) {
-    float4 v;
-    asm volatile("ld.global.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-                 : "l"(p), "l"(pol)
+// 16 bytes global -> shared without passing through registers (completed by cp_async_wait)
+__device__ __forceinline__ void cp_async16_keep(float *dst, const float *src, uint64_t pol) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "l"(pol)
                  : "memory");
-    return v;
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// A hint to bring [p, p + bytes) into L2 (16-byte aligned, a multiple of 16 bytes); nothing
+// waits for it.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
 struct Params {
@@ -460,22 +472,39 @@ __device__ __forceinline__ void eval_chunk(const Params &p, uint32_t r, f3 o, f3
     const int q = lane % kL;
     const uint32_t sy = R1, sz = R1 * R1;
     [[maybe_unused]] const uint64_t nv = (uint64_t)R1 * R1 * R1;  // vertex rows
+#if QSDVR_GATHER_PREFETCH
+    if constexpr (QSDVR_GATHER_PREFETCH == 2 || kDeg == 2) {
+        // samples of the gather's first round of loads (issued right below) are not prefetched
+        constexpr int kRound = (sizeof(S) == 2 ? GatherLanes<S, kDeg>::kPerStep : kPS) * kGatherUnroll;
+        if (!from_slot && s.shaded && lane >= kRound) {
+            constexpr uint32_t kPair = 2u * kC * sizeof(S);  // rows v and v + 1 are adjacent
+            const S *base = static_cast<const S *>(p.data);
+            const uint32_t pv[4] = {s.vbase, s.vbase + sy, s.vbase + sz, s.vbase + sz + sy};
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                prefetch_l2(QSDVR_AT(base, (uint64_t)kC * pv[t], 2 * kC, (uint64_t)kC * nv), kPair);
+        }
+    }
+#endif
     if (!from_slot) {
         st4(tile + lane * kRow + kC, make_float4(__uint_as_float(s.shaded ? s.vbase : kNoVertex), s.wx, s.wy, s.wz));
         __syncwarp();
     }
     if (from_slot) {
-        // rows stashed by the forward, one row per kL lanes per warp instruction
+        // rows stashed by the forward, one row per kL lanes per step, copied into the tile by
+        // asynchronous 16-byte copies that are all in flight at once (one L2 round trip per
+        // chunk instead of one per round of register loads)
         const uint64_t pol = evict_last_policy();
-#pragma unroll 2
+#pragma unroll
         for (int st = 0; st < kL; ++st) {
             const int j = st * kPS + lane / kL;
-            st4(tile + j * kRow + 4 * q, ld4_keep(from_slot + j * kC + 4 * q, pol));
+            cp_async16_keep(tile + j * kRow + 4 * q, from_slot + j * kC + 4 * q, pol);
         }
+        cp_async_wait();
 #if QSDVR_STASH_DISCARD
         // The stash is dead once read: drop its L2 lines without writing them back (they
         // would otherwise reach DRAM as dirty evictions) and free the room for the gathers.
-        // The tile stores above consumed every loaded value, so the loads are complete.
+        // Every lane's copies have completed (cp.async.wait_all before the warp barrier).
         __syncwarp();
         constexpr uint32_t kLines = kWarp * kC * sizeof(float) / 128;  // the chunk's 128-byte lines
         for (uint32_t l = lane; l < kLines; l += kWarp)
@@ -1444,11 +1473,15 @@ __global__ void __launch_bounds__(256) ray_order_keys_kernel(const qsdvr_ray_inf
 // not change what the rays in flight share.
 constexpr uint32_t kOrderBuckets = (1u << 15) + 1;
 
+// With a sample list (list mode) the key point is each ray's median SDF position instead: the
+// fine samples gather where the compositing weights are, so rays keyed there run beside the
+// rays that hit the same patch of the surface and share its vertex rows and gradient lines.
 __device__ __forceinline__ uint32_t ray_bucket(const qsdvr_ray_info *rays, const float *origin, const float *dir,
-                                               uint32_t r, float interval) {
+                                               uint32_t r, uint32_t n, float interval, const float *tlist) {
     const uint32_t ns = rays[r].sdf_count;
     if (ns < 2) return kOrderBuckets - 1;
-    const float t = 0.5f * (float)(ns - 1) * interval;
+    const float t = tlist ? *QSDVR_AT(tlist, (uint64_t)kListT * r + kListT / 2, 1, (uint64_t)kListT * n)
+                          : 0.5f * (float)(ns - 1) * interval;
     const f3 o = load3(origin + 3ull * r), d = load3(dir + 3ull * r);
     const float c[3] = {fmaf(d.x, t, o.x), fmaf(d.y, t, o.y), fmaf(d.z, t, o.z)};
     uint32_t q[3];
@@ -1460,10 +1493,11 @@ __device__ __forceinline__ uint32_t ray_bucket(const qsdvr_ray_info *rays, const
 __global__ void __launch_bounds__(256) ray_bucket_kernel(const qsdvr_ray_info *__restrict__ rays,
                                                          const float *__restrict__ origin,
                                                          const float *__restrict__ dir, uint32_t n, float interval,
-                                                         uint32_t *__restrict__ bucket, uint32_t *__restrict__ hist) {
+                                                         const float *__restrict__ tlist, uint32_t *__restrict__ bucket,
+                                                         uint32_t *__restrict__ hist) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
-    const uint32_t b = ray_bucket(rays, origin, dir, r, interval);
+    const uint32_t b = ray_bucket(rays, origin, dir, r, n, interval, tlist);
     bucket[r] = b;
     atomicAdd(hist + b, 1u);
 }
@@ -1545,25 +1579,43 @@ extern "C" size_t qsdvr_ray_order_workspace_size(uint32_t ray_count) {
     return ((size_t)kOrderBuckets + (size_t)ray_count) * sizeof(uint32_t);
 }
 
+namespace qsdvr {
+namespace {
+int ray_order(const char *fn, const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
+              float interval, const float *tlist, uint32_t *order, void *workspace, size_t workspace_bytes,
+              cudaStream_t stream) {
+    if (ray_count == 0) return QSDVR_OK;
+    if (!rays || !origin || !dir || !order) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "%s: null pointer", fn);
+    if (!tlist && !(interval > 0.0f)) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "%s: interval must be > 0", fn);
+    const size_t need = qsdvr_ray_order_workspace_size(ray_count);
+    if (!workspace || workspace_bytes < need || !aligned(workspace, 4))
+        return set_error(QSDVR_ERR_WORKSPACE, "%s: workspace %zu < %zu bytes (4-byte aligned)", fn, workspace_bytes,
+                         need);
+    uint32_t *hist = static_cast<uint32_t *>(workspace), *bucket = hist + kOrderBuckets;
+    const int st = check_cuda(cudaMemsetAsync(hist, 0, kOrderBuckets * sizeof(uint32_t), stream), fn);
+    if (st != QSDVR_OK) return st;
+    const unsigned blocks = grid_for(ray_count, 256);
+    ray_bucket_kernel<<<blocks, 256, 0, stream>>>(rays, origin, dir, ray_count, interval, tlist, bucket, hist);
+    bucket_scan_kernel<<<1, 1024, 0, stream>>>(hist);
+    ray_scatter_kernel<<<blocks, 256, 0, stream>>>(bucket, ray_count, hist, order);
+    return check_launch(fn);
+}
+}  // namespace
+}  // namespace qsdvr
+
 extern "C" int qsdvr_ray_order(const qsdvr_ray_info *rays, const float *origin, const float *dir, uint32_t ray_count,
                                float interval, uint32_t *order, void *workspace, size_t workspace_bytes,
                                cudaStream_t stream) {
-    if (ray_count == 0) return QSDVR_OK;
-    if (!rays || !origin || !dir || !order)
-        return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_order: null pointer");
-    if (!(interval > 0.0f)) return set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_order: interval must be > 0");
-    const size_t need = qsdvr_ray_order_workspace_size(ray_count);
-    if (!workspace || workspace_bytes < need || !aligned(workspace, 4))
-        return set_error(QSDVR_ERR_WORKSPACE, "qsdvr_ray_order: workspace %zu < %zu bytes (4-byte aligned)",
-                         workspace_bytes, need);
-    uint32_t *hist = static_cast<uint32_t *>(workspace), *bucket = hist + kOrderBuckets;
-    const int st = check_cuda(cudaMemsetAsync(hist, 0, kOrderBuckets * sizeof(uint32_t), stream), "qsdvr_ray_order: memset");
-    if (st != QSDVR_OK) return st;
-    const unsigned blocks = grid_for(ray_count, 256);
-    ray_bucket_kernel<<<blocks, 256, 0, stream>>>(rays, origin, dir, ray_count, interval, bucket, hist);
-    bucket_scan_kernel<<<1, 1024, 0, stream>>>(hist);
-    ray_scatter_kernel<<<blocks, 256, 0, stream>>>(bucket, ray_count, hist, order);
-    return check_launch("qsdvr_ray_order");
+    return qsdvr::ray_order("qsdvr_ray_order", rays, origin, dir, ray_count, interval, nullptr, order, workspace,
+                            workspace_bytes, stream);
+}
+
+extern "C" int qsdvr_ray_order_list(const qsdvr_ray_info *rays, const float *origin, const float *dir,
+                                    uint32_t ray_count, const float *tlist, uint32_t *order, void *workspace,
+                                    size_t workspace_bytes, cudaStream_t stream) {
+    if (ray_count && !tlist) return qsdvr::set_error(QSDVR_ERR_INVALID_ARGUMENT, "qsdvr_ray_order_list: null tlist");
+    return qsdvr::ray_order("qsdvr_ray_order_list", rays, origin, dir, ray_count, 0.0f, tlist, order, workspace,
+                            workspace_bytes, stream);
 }
 
 namespace {

@@ -46,6 +46,7 @@ _lib.extra_signatures({
     "qsdvr_ray_order_keys": [P, P, P, U32, F32, P, P],
     "qsdvr_sdf_cells_bf16": [P, P, ctypes.c_uint64, P],
     "qsdvr_ray_order": [P, P, P, U32, F32, P, P, ctypes.c_size_t, P],
+    "qsdvr_ray_order_list": [P, P, P, U32, P, P, P, ctypes.c_size_t, P],
     "qsdvr_render_forward_bricks": [ctypes.POINTER(RenderArgs), P],
 }, {"qsdvr_render_workspace_size": [ctypes.POINTER(RenderArgs)], "qsdvr_ray_order_workspace_size": [U32]})
 
@@ -133,8 +134,7 @@ def make_args(rays, origin, direction, sdf_grid, data, reso, interval, k, mode="
     a.merge_scatter = 1 if merge else 0
     a.workspace, a.workspace_bytes = None, 0
     if tlist is not None:
-        if tlist.device != dev or tlist.dtype != torch.float32 or tlist.shape != (n, 33) or not tlist.is_contiguous():
-            raise ValueError(f"tlist must be a contiguous float32 [N,33] tensor on {dev}")
+        _check_tlist(tlist, n, dev)
         a.tlist = tlist.data_ptr()
     if sample_alpha is not None:
         if sample_alpha.device != dev or sample_alpha.dtype != torch.float32 or not sample_alpha.is_contiguous():
@@ -160,13 +160,22 @@ def _stream(dev):
     return ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
 
 
-def ray_order(rays, origin, direction, interval) -> torch.Tensor:
+def _check_tlist(tlist, n, dev):
+    if tlist.device != dev or tlist.dtype != torch.float32 or tlist.shape != (n, 33) or not tlist.is_contiguous():
+        raise ValueError(f"tlist must be a contiguous float32 [N,33] tensor on {dev}")
+
+
+def ray_order(rays, origin, direction, interval, tlist=None) -> torch.Tensor:
     """A permutation (int32 [N]) that lists the rays by the Morton code of their in-box
     midpoint on a 32^3 lattice (qsdvr_ray_order: the library's counting sort), rays without
     samples last.  Passed as ``order`` to the render calls, neighbouring rays in the kernel's
     schedule cross neighbouring cells, so more of the gathered rows and gradient lines are found
-    in L2."""
+    in L2.  With ``tlist`` (the [N,33] sample list of a list-mode render) each ray is keyed on
+    its median SDF position instead (qsdvr_ray_order_list), so rays that hit the same patch of
+    the surface run side by side."""
     dev, n = _check_batch(rays, origin, direction)
+    if tlist is not None:
+        _check_tlist(tlist, n, dev)
     order = torch.empty(n, dtype=torch.int32, device=dev)
     if n == 0:
         return order
@@ -177,8 +186,12 @@ def ray_order(rays, origin, direction, interval) -> torch.Tensor:
         ws = torch.empty(need, dtype=torch.uint8, device=dev)
         _workspaces[key] = ws
     with torch.cuda.device(dev):
-        call("qsdvr_ray_order", _ptr(rays), _ptr(origin), _ptr(direction), n, float(interval), _ptr(order),
-             ws.data_ptr(), ws.numel(), _stream(dev))
+        if tlist is None:
+            call("qsdvr_ray_order", _ptr(rays), _ptr(origin), _ptr(direction), n, float(interval), _ptr(order),
+                 ws.data_ptr(), ws.numel(), _stream(dev))
+        else:
+            call("qsdvr_ray_order_list", _ptr(rays), _ptr(origin), _ptr(direction), n, _ptr(tlist), _ptr(order),
+                 ws.data_ptr(), ws.numel(), _stream(dev))
     return order
 
 

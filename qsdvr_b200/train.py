@@ -171,7 +171,7 @@ def run(a, data=None, quiet=False, return_state=False):
                             points=a.proposal_points)
             if a.proposal and step > a.proposal_warmup:
                 tlist = net.sample(r, o, d, a.interval, a.proposal_mix)
-        order = fused.ray_order(r, o, d, a.interval) if a.ray_order else None
+        order = fused.ray_order(r, o, d, a.interval, tlist=tlist) if a.ray_order else None
         fused.render_train(tg, r, o, d, sg, dg, R, a.interval, a.k, model.sdfGrid.grad, data_grad,
                            a.mode, model.transmittance, loss=loss, tlist=tlist, order=order)
         e1.record()

@@ -271,6 +271,52 @@ def test_list_render_vs_oracle(prop, sh):
     assert rel_err(sg2.cpu(), sg.cpu()) < 1e-5 and rel_err(dg2.cpu(), dg.cpu()) < 1e-5
 
 
+def test_list_ray_order(prop):
+    """qsdvr_ray_order_list: a permutation of the batch listing the rays by the 15-bit Morton
+    code (32^3 lattice) of the point at their median SDF position tlist[:, 16], rays without
+    samples last; a list-mode training launch taken in that order gives the batch order's
+    colours, loss and gradients."""
+    from qsdvr_b200 import _lib, fused, scenes
+
+    R, k, interval = 24, 10.0, 4.0 / 128
+    cam = _camera((1.7, -3.3, 1.5), 40, 55.0, interval, R)
+    grid8 = fused.pad_grid7(scenes.sphere_grid(R, 0.55, 0.01, seed=35).reshape(-1, 7)).to(DEV)
+    data = scenes.appearance(R, seed=35).to(DEV)
+    rays = cam.rayList.cpu().numpy()
+    n = rays.shape[0]
+    tl = _random_tlist(rays, interval, 36)
+    tl_d = torch.from_numpy(tl).to(DEV)
+    args = (cam.rayList, cam.originList, cam.dirList)
+    order = fused.ray_order(*args, interval, tlist=tl_d)
+    assert torch.equal(order.sort().values.cpu(), torch.arange(n, dtype=torch.int32))
+    o, d = cam.originList.cpu().numpy(), cam.dirList.cpu().numpy()
+    ns = rays[:, 0].astype(np.int64)
+    pt = o + d * tl[:, 16:17]
+    q = np.clip(np.floor((pt + 1.0) * 16.0), 0, 31).astype(np.int64)
+    key = np.zeros(n, np.int64)
+    for b in range(5):
+        for a in range(3):
+            key |= ((q[:, a] >> b) & 1) << (3 * b + a)
+    key[ns < 2] = 1 << 15
+    ks = key[order.cpu().numpy()]
+    # (float rounding at lattice edges aside; rays without samples carry the largest key)
+    assert np.mean(np.diff(ks) >= 0) > 0.999
+    target = torch.rand((n, 3), generator=torch.Generator().manual_seed(37)).to(DEV)
+    out = []
+    for o_ in (None, order):
+        sg, dg = torch.zeros_like(grid8), torch.zeros_like(data)
+        col, loss = fused.render_train(target, *args, grid8, data, R, interval, k, sg, dg, mode="fixed",
+                                       tlist=tl_d, order=o_)
+        out.append((col, loss, sg, dg))
+    (c0, l0, s0, d0), (c1, l1, s1, d1) = out
+    assert (c0 - c1).abs().max().item() < 1e-6
+    assert abs(l0.item() - l1.item()) <= n * 2.0 ** -24 * max(1.0, l0.item())
+    assert rel_err(s1.cpu(), s0.cpu()) < 1e-5 and rel_err(d1.cpu(), d0.cpu()) < 1e-5
+    assert _lib.device_error() == 0
+    with pytest.raises(ValueError):
+        fused.ray_order(*args, interval, tlist=tl_d[:, :32].contiguous())
+
+
 def test_sample_alpha_matches_oracle(prop):
     from qsdvr_b200 import fused, scenes
 
