@@ -829,6 +829,21 @@ def _cpu_step(grid7, data, batch_cpu, R, interval):
     return float(loss)
 
 
+def _oracle_step(grid7, data, batch_cpu, R, interval):
+    """The same fwd+bwd by the float64 vectorised oracle (oracle/oracle.py, torch autograd)."""
+    import oracle.oracle as O
+
+    pts = O.generate_ray_points(batch_cpu["rays"], batch_cpu["origin"], batch_cpu["dir"], interval, R)
+    inp = {k: torch.from_numpy(v) for k, v in pts.items()}
+    inp["rayList"] = torch.from_numpy(batch_cpu["rays_packed"].astype(np.int64))
+    g = grid7.detach().double().requires_grad_()
+    d = data.detach().double().requires_grad_()
+    img = O.render(g, d, inp, K_LOGISTIC, compat=True)
+    loss = ((img - batch_cpu["target"].double()) ** 2).mean()
+    loss.backward()
+    return float(loss)
+
+
 def _cpu_batch(batch, n):
     """First n rays of a batch, repacked with fresh sample offsets (host arrays)."""
     rays = batch["rays"][:n].cpu().numpy().view(np.uint32).copy()
@@ -928,6 +943,12 @@ def run_reference(args, cfg):
         _cpu_step(grid7, data_cpu, b, cfg["R"], cfg["interval"])
     dt = time.perf_counter() - t0
     value = n * args.steps / dt
+    # the float64 oracle on the same sample, one step after a warm-up: reported beside the
+    # baseline, not as it
+    _oracle_step(grid7, data_cpu, b, cfg["R"], cfg["interval"])
+    t1 = time.perf_counter()
+    _oracle_step(grid7, data_cpu, b, cfg["R"], cfg["interval"])
+    oracle_rays_per_s = n / (time.perf_counter() - t1)
     samples = int(np.maximum(b["rays"][:, 0].astype(np.int64) - 1, 0).sum())
     full = cfg.get("scene") == "sphere"
     sample = (f"all {n} rays of the view ({samples} render samples)" if full else
@@ -944,7 +965,10 @@ def run_reference(args, cfg):
                              "kind": "port",
                              "sample": f"{sample}; reference torch render path (models/render_torch.py, per-ray "
                                        f"loop) fwd+bwd on the host; os.cpu_count()={os.cpu_count()}"},
-            "e2e": {"value": round(value, 2), "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": round(value, 2), "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "oracle_timing": {"value": round(oracle_rays_per_s, 2), "unit": "rays/s",
+                              "label": "oracle, not the baseline: the float64 vectorised restatement "
+                                       "(oracle/oracle.py, compat mode, torch autograd) fwd+bwd on the same sample"}}
     print(json.dumps(line))
 
 
