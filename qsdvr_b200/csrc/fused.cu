@@ -1502,16 +1502,29 @@ __global__ void __launch_bounds__(256) ray_bucket_kernel(const qsdvr_ray_info *_
     atomicAdd(hist + b, 1u);
 }
 
-// Exclusive scan of the kOrderBuckets counts in place, one block of 1024 threads.
+// Exclusive scan of the kOrderBuckets counts in place, one block of 1024 threads.  Each
+// thread scans kPer consecutive counts; they pass through shared memory so that the global
+// loads and stores are coalesced (thread t's run read straight from global memory touched a
+// different sector per thread and step), and the stride-kPer shared accesses (kPer odd) fall
+// in distinct banks.
+constexpr uint32_t kScanPer = (kOrderBuckets + 1023) / 1024;
+constexpr size_t kScanSmem = (size_t)kScanPer * 1024 * sizeof(uint32_t);
 __global__ void __launch_bounds__(1024) bucket_scan_kernel(uint32_t *__restrict__ hist) {
-    constexpr uint32_t kPer = (kOrderBuckets + 1023) / 1024;
+    constexpr uint32_t kPer = kScanPer;
+    static_assert(kPer % 2 == 1, "an odd run length keeps the shared accesses conflict-free");
+    extern __shared__ uint32_t counts[];  // kPer * 1024
     __shared__ uint32_t warp_sums[32];
     const uint32_t t = threadIdx.x, lane = t & 31, w = t >> 5;
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+        const uint32_t i = k * 1024 + t;
+        counts[i] = i < kOrderBuckets ? hist[i] : 0u;
+    }
+    __syncthreads();
     uint32_t v[kPer], sum = 0;
 #pragma unroll
     for (uint32_t k = 0; k < kPer; ++k) {
-        const uint32_t i = t * kPer + k;
-        v[k] = i < kOrderBuckets ? hist[i] : 0u;
+        v[k] = counts[t * kPer + k];
         sum += v[k];
     }
     uint32_t incl = sum;
@@ -1535,9 +1548,14 @@ __global__ void __launch_bounds__(1024) bucket_scan_kernel(uint32_t *__restrict_
     uint32_t run = warp_sums[w] + incl - sum;
 #pragma unroll
     for (uint32_t k = 0; k < kPer; ++k) {
-        const uint32_t i = t * kPer + k;
-        if (i < kOrderBuckets) hist[i] = run;
+        counts[t * kPer + k] = run;
         run += v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; ++k) {
+        const uint32_t i = k * 1024 + t;
+        if (i < kOrderBuckets) hist[i] = counts[i];
     }
 }
 
@@ -1594,9 +1612,14 @@ int ray_order(const char *fn, const qsdvr_ray_info *rays, const float *origin, c
     uint32_t *hist = static_cast<uint32_t *>(workspace), *bucket = hist + kOrderBuckets;
     const int st = check_cuda(cudaMemsetAsync(hist, 0, kOrderBuckets * sizeof(uint32_t), stream), fn);
     if (st != QSDVR_OK) return st;
+    // (the scan's shared memory is above the default 48 KB; the attribute is set on the
+    // current device at every call: it is a host-side setting, not a stream operation)
+    const int sa = check_cuda(
+        cudaFuncSetAttribute(bucket_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScanSmem), fn);
+    if (sa != QSDVR_OK) return sa;
     const unsigned blocks = grid_for(ray_count, 256);
     ray_bucket_kernel<<<blocks, 256, 0, stream>>>(rays, origin, dir, ray_count, interval, tlist, bucket, hist);
-    bucket_scan_kernel<<<1, 1024, 0, stream>>>(hist);
+    bucket_scan_kernel<<<1, 1024, kScanSmem, stream>>>(hist);
     ray_scatter_kernel<<<blocks, 256, 0, stream>>>(bucket, ray_count, hist, order);
     return check_launch(fn);
 }
